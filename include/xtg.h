@@ -1,0 +1,177 @@
+/*
+ * xtg.h -- C ABI of libxtgpu.so, the B200 TIMBIR/MBIR reconstruction core.
+ *
+ * The reference engine (gromitsun/timbir-python Source_Code_4D_Fast) is one C
+ * program whose hot path is ICD_BackProject and the routines under it.  This
+ * library replaces those routines; the host program XT_Engine (same command
+ * line, same files) calls it through the entry points below.  Each entry
+ * point names the reference routine it replaces.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Host arrays are row-major float32 in the
+ *     reference's layouts:
+ *       sinogram arrays (projection y, weight w, error e)  [N_p][N_r][N_t]
+ *       projection offset d                                [N_r][N_t]
+ *       object x                                           [N_time][N_z][N_y][N_x]
+ *       magnitude-update map                               [N_time][nzb][N_y][N_x]
+ *   - Every call returns 0 or a negative XTG_E* status; xtg_last_error()
+ *     gives the message.  No exception crosses the ABI.  A context is not
+ *     thread safe; use one context per host thread.
+ *   - All device state lives in one context on the current CUDA device; the
+ *     library never falls back to the CPU: without a usable sm_100 GPU,
+ *     xtg_create fails with XTG_E_CUDA.
+ */
+#ifndef XTG_H
+#define XTG_H
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../timbir-python_b200/csrc/xt_geom.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XTG_ABI_VERSION 1
+
+enum {
+  XTG_OK = 0,
+  XTG_E_ARG = -1,     /* bad argument or configuration */
+  XTG_E_CUDA = -2,    /* CUDA runtime error (no device, out of memory, launch failure) */
+  XTG_E_STATE = -3,   /* call out of order (e.g. iterate before the sinogram is uploaded) */
+  XTG_E_NUMERIC = -4, /* non-finite value met in an update (theta2 <= 0 with zero prior weight) */
+  XTG_E_TIMEOUT = -5  /* a bounded device-side wait gave up */
+};
+
+/* A-matrix storage used by the ICD kernel.
+ *   XTG_A_FP32: entries computed on the fly from H_r, bit-identical to
+ *               calcAMatrixColumnforAngle (XT_AMatrix.c:50-110).
+ *   XTG_A_FP16: entries precomputed once per context into HBM as FP16 with
+ *               one FP32 scale per (frame, column). */
+enum { XTG_A_FP32 = 0, XTG_A_FP16 = 1 };
+
+/* Update order.
+ *   XTG_ORDER_PARALLEL: many columns in flight at once (the B200 schedule);
+ *   XTG_ORDER_SEQUENTIAL: one column at a time, slices in increasing z, in
+ *       the list order given -- the reference's own order, for parity tests. */
+enum { XTG_ORDER_PARALLEL = 0, XTG_ORDER_SEQUENTIAL = 1 };
+
+typedef struct xtg_ctx xtg_ctx;
+
+/* Per-iteration statistics, the quantities updateVoxelsTimeSlices logs and
+ * tests (XT_ICD_update.c:884-925). */
+typedef struct {
+  double avg_update_pct;   /* 100 * sum(MagUpdateMap over the random lists) / vox_mag */
+  double mag_sum;          /* sum of MagUpdateMap over the random lists */
+  double vox_mag;          /* sum |x| over voxels updated in the last chunk's random pass */
+  double total_pix;        /* voxels in the random lists */
+  int64_t voxel_updates;   /* voxel updates performed (random + NHICD), zero-skipped excluded */
+  int64_t zero_skipped;    /* voxels skipped by ZERO_SKIPPING */
+  int64_t columns;         /* column (z-line) work items processed */
+  int32_t converged;       /* avg_update_pct < voxel_thresh */
+  float ms;                /* device time of the iteration, CUDA events */
+} xtg_stats;
+
+/* Replaces argsParser/initStructures/DetectorResponseProfile set-up
+ * (XT_Init.c:277-629, XT_Profile.c:128-217, XT_ICD_update.c:952-978).
+ * view_times / view_angles_deg: the n entries of view_info.txt. */
+int xtg_create(const xt_params *prm, const double *view_times, const double *view_angles_deg, int32_t n,
+               xtg_ctx **out);
+void xtg_destroy(xtg_ctx *ctx);
+const char *xtg_last_error(void);
+int xtg_abi_version(void);
+
+/* dims[]: N_x, N_y, N_z, N_time, N_r, N_t, N_p, nzb, zovl, amax */
+int xtg_dims(const xtg_ctx *ctx, int32_t *dims);
+/* Geometry and tables exactly as the GPU uses them (host copies). */
+int xtg_geometry(const xtg_ctx *ctx, xt_geom *g);
+int xtg_get_hr(const xtg_ctx *ctx, float *hr /*[N_p][65]*/);
+
+/* Options: A storage, update order, concurrent columns (0 = device default),
+ * seed of the GPU visiting order. */
+int xtg_set_options(xtg_ctx *ctx, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed);
+
+/* genSinogram_fromBin + computeWriteSinogram (XT_genSinogram.c:264-300,
+ * XT_Engine.c:89-121): y, w and the offset d (NULL = zero).  Weights are
+ * divided by the variance estimate on the device, like the reference. */
+int xtg_upload_sino(xtg_ctx *ctx, const float *y, const float *w, const float *d);
+/* Counts ingest, genSinogram_subsampleCounts (XT_genSinogram.c:303-374):
+ * bright [N_r*mult_xy][N_t*mult_z] and weight counts [N_p][N_r*mult_xy][N_t*mult_z]
+ * are binned to y = log(bright/counts) (+ BH_QUAD_COEF * y^2) and w = counts. */
+int xtg_upload_counts(xtg_ctx *ctx, const float *bright, const float *counts, double bh_quad_coef,
+                      const float *d);
+int xtg_upload_object(xtg_ctx *ctx, const float *x);
+int xtg_download_object(xtg_ctx *ctx, float *x);
+int xtg_get_error_sino(xtg_ctx *ctx, float *e);
+int xtg_set_error_sino(xtg_ctx *ctx, const float *e);
+int xtg_get_weight(xtg_ctx *ctx, float *w);
+int xtg_get_offset(xtg_ctx *ctx, float *d);
+int xtg_set_offset(xtg_ctx *ctx, const float *d);
+int xtg_get_magmap(xtg_ctx *ctx, float *m);
+int xtg_set_magmap(xtg_ctx *ctx, const float *m);
+int xtg_get_variance(xtg_ctx *ctx, double *var_est);
+int xtg_set_variance(xtg_ctx *ctx, double var_est);
+
+/* A-matrix column generation on the GPU, calcAMatrixColumnforAngle
+ * (XT_AMatrix.c:50-110), for n (row, col, view) triples.  vals/idx hold amax
+ * slots per triple, cnt the entry count. */
+int xtg_amatrix(xtg_ctx *ctx, int32_t n, const int32_t *rows, const int32_t *cols, const int32_t *views,
+                float *vals, int32_t *idx, int32_t *cnt);
+/* Forward projection A x of the current object, FP32, summed in the
+ * reference's order (initErrorSinogam + forward_project_voxel_AMat1D,
+ * XT_ICD_update.c:551-569, XT_ForwardProject.c:8-25).  ax may be NULL
+ * (result stays on the device). */
+int xtg_forward_project(xtg_ctx *ctx, float *ax);
+/* e = y - A x - d in FP32 (initErrorSinogam, XT_ICD_update.c:538-597). */
+int xtg_init_error_sino(xtg_ctx *ctx);
+/* e = y - A x - d with FP64 accumulation, rounded to FP32: the periodic
+ * resync that removes the drift of incremental FP32 updates.  The same pass
+ * yields the MAP cost of the current object in FP64 (outputs may be NULL). */
+int xtg_resync_fp64(xtg_ctx *ctx, double *cost, double *forward, double *prior);
+/* MAP cost of the current object (computeCost, XT_ICD_update.c:181-314),
+ * evaluated in FP64 from e64 = y - A x - d (not from the running e). */
+int xtg_map_cost_fp64(xtg_ctx *ctx, double *cost, double *forward, double *prior);
+/* MAP cost from the running error sinogram in FP64 arithmetic. */
+int xtg_map_cost_running(xtg_ctx *ctx, double *cost, double *forward, double *prior);
+
+/* Zinger weight refresh: ProjSelect = |e sqrt(w)| < T for every sinogram
+ * entry (XT_ICD_update.c:576-580, 659-663, 750-753; XT_VoxUpdate.c:76-79).
+ * sel (may be NULL) receives the mask; nsel the count of selected entries. */
+int xtg_zinger_refresh(xtg_ctx *ctx, uint8_t *sel, int64_t *nsel);
+
+/* One reference iteration, updateVoxelsTimeSlices (XT_ICD_update.c:767-926):
+ * a random visiting order cut in 10 chunks, each chunk followed by NHICD
+ * selection and (iter > 1, NHICD on) an NHICD pass; offset and variance
+ * updates when enabled.  Voxels of a column's z-line are updated together. */
+int xtg_icd_iteration(xtg_ctx *ctx, int32_t iter, xtg_stats *st);
+
+/* Column update over an explicit work list (the hot kernel alone):
+ * items[4*q] = {frame, row, col, block}, block = -1 for the whole z-line.
+ * Used by the sequential parity tests and the benchmark. */
+int xtg_update_columns(xtg_ctx *ctx, int32_t iter, int32_t n_items, const int32_t *items, xtg_stats *st);
+
+/* NHICD selection, VSC_based_Voxel_Line_Select + ComputeVSC
+ * (XT_NHICD.c:128-216): 5x5 Hamming filter of the magnitude-update map, the
+ * order statistic at N_xy - floor(update_select_num/10), the columns above it.
+ * update_select_num[N_time*nzb] in; nhicd_num[N_time*nzb] and, when not
+ * NULL, the lists (x, y) [N_time][nzb][N_xy] out (raster order). */
+int xtg_nhicd_select(xtg_ctx *ctx, const int32_t *update_select_num, int32_t *nhicd_num, int32_t *x_sel,
+                     int32_t *y_sel, float *thresholds);
+
+/* update_Sinogram_Offset (XT_ICD_update.c:666-759) and
+ * update_variance_parameter (XT_ICD_update.c:633-664). */
+int xtg_update_offset(xtg_ctx *ctx);
+int xtg_update_variance(xtg_ctx *ctx);
+
+/* Device bytes held by the context. */
+int64_t xtg_device_bytes(const xtg_ctx *ctx);
+/* Kernel launches issued by this context since creation (all kernels). */
+int64_t xtg_launch_count(const xtg_ctx *ctx);
+/* Device time (ms) of the ICD column kernel in the last xtg_icd_iteration /
+ * xtg_update_columns call, and the column work items it processed. */
+int xtg_last_kernel_time(const xtg_ctx *ctx, float *ms, int64_t *items, int64_t *rows_touched);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,169 @@
+"""Generates the golden fixtures in tests/golden from the reference itself.
+
+Runs the reference engine's own routines (gromitsun/timbir-python
+Source_Code_4D_Fast, compiled by `make -C oracle` into oracle/_ref) on small
+seeded cases and stores inputs and outputs as .npz files.  The CPU tests pin
+the oracle restatement (oracle/xt_oracle.c) against these files, so the pin
+holds on machines without the reference tree.
+
+    python tests/golden/make_golden.py      # needs oracle/_ref (this container)
+
+The RNG known-answer table is read from the reference source's own comment
+(Source_Code_4D_Fast/randlib.c:69-91) and checked against the compiled
+generator before it is stored.
+"""
+import os
+import re
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "timbir-python_b200"), os.path.join(ROOT, "tests")]
+
+import common  # noqa: E402
+import xtg  # noqa: E402
+from oracle.oracle import Reference, ref_available  # noqa: E402
+
+REF_SRC = "/root/reference/Source_Code_4D_Fast/randlib.c"
+
+CASES = {
+    # name: (params kwargs, view kind, data kwargs, iterations)
+    "plain3d": (dict(N=32, NT=4, NP=36), None, dict(seed=1), 3),
+    "zinger_nhicd": (dict(N=24, NT=4, NP=30, zinger=True, nhicd=True, offset=2, var=1), None,
+                     dict(seed=2, zfrac=0.01), 4),
+    "offset_zero_mean": (dict(N=20, NT=2, NP=24, offset=2, zero_mean=1, zinger=True), None,
+                         dict(seed=6, zfrac=0.02), 2),
+    "timbir4d": (dict(N=16, NT=2, NP=48, n_time=3), (4, 16), dict(seed=3, moving=2), 3),
+    "blocks_z": (dict(N=16, NT=8, NP=20, threads=4, nhicd=True), None, dict(seed=4), 3),
+    "coarse_xy2": (dict(N=32, NT=4, NP=30, dxy=2.0, dz=2.0), None, dict(seed=5), 2),
+}
+
+
+def run_case(name, pk, vk, dk, iters, double=False):
+    p = common.params(**pk)
+    with tempfile.TemporaryDirectory() as d:
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            t, a = common.views(p, vk)
+            xtg.write_view_file("view_info.txt", t, a)
+            x, ax, y, w = common.data(p, t, a, **dk)
+            r = Reference(p, double=double)
+            out = dict(times=t, angles=a, y=y, w=w, x_true=x, ax=ax)
+            out["derived"] = r.derived()
+            out["hr"] = r.hr()
+            v, cs, sn, pn, pi = r.views()
+            out.update(view_rad=v, cosv=cs, sinv=sn, proj_num=pn, proj_idx=pi)
+            rng = np.random.default_rng(11)
+            trip = np.stack([rng.integers(0, r.N_y, 400), rng.integers(0, r.N_x, 400),
+                             rng.integers(0, r.N_p, 400)], 1).astype(np.int32)
+            av = np.zeros((400, 16), r.real)
+            ai = np.full((400, 16), -1, np.int32)
+            for q, (row, col, view) in enumerate(trip):
+                vals, idx = r.amatrix(int(row), int(col), int(view))
+                av[q, :len(vals)] = vals
+                ai[q, :len(idx)] = idx
+            out.update(a_trip=trip, a_vals=av, a_idx=ai)
+            r.set_sino(y, w)
+            r.set_object(x)
+            r.init_error_sino()
+            out["e_true"] = r.error_sino()
+            out["cost_true"] = np.array(r.cost())
+            r.set_object(np.zeros(r.obj_shape, r.real))
+            r.init_error_sino()
+            out["cost_0"] = np.array(r.cost())
+            r.srandom2(761521)
+            objs, costs, offs, vars_, mags = [], [], [], [], []
+            for it in range(1, iters + 1):
+                r.iterate(it)
+                objs.append(r.object())
+                costs.append(r.cost())
+                offs.append(r.offset())
+                vars_.append(r.var())
+                mags.append(r.magmap())
+            out.update(objs=np.array(objs), costs=np.array(costs), offsets=np.array(offs), vars=np.array(vars_),
+                       magmaps=np.array(mags), e_final=r.error_sino())
+            r.close()
+        finally:
+            os.chdir(cwd)
+    return out
+
+
+def rng_kat():
+    txt = open(REF_SRC).read()
+    blk = txt[txt.index("TABLE:"):txt.index("Test for verifying")]
+    table = np.array([int(s) for s in re.findall(r"^\s*(\d+)\s*$", blk, re.M)], np.int64)
+    assert len(table) == 20, table
+    p = common.params()
+    with tempfile.TemporaryDirectory() as d:
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            xtg.write_view_file("view_info.txt", *common.views(p))
+            r = Reference(p)
+            r.srandom2(1)
+            got = np.array([round(r.random2() * 2147483647) for _ in range(20)], np.int64)
+            r.close()
+        finally:
+            os.chdir(cwd)
+    assert np.array_equal(got, table), (got, table)
+    return table
+
+
+def nhicd_case():
+    p = common.params(N=32, NT=8, NP=12, threads=2)
+    with tempfile.TemporaryDirectory() as d:
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            xtg.write_view_file("view_info.txt", *common.views(p))
+            r = Reference(p)
+            rng = np.random.default_rng(5)
+            m = rng.random((r.N_time, r.nzb, r.N_y, r.N_x)).astype(np.float32)
+            m[m < 0.3] = 0.0
+            m[:, :, 3, 4:9] = 0.75  # ties
+            r.set_magmap(m)
+            usn = np.full(r.N_time * r.nzb, 700, np.int32)
+            r.srandom2(99)
+            nn, xs, ys = r.nhicd_select(usn)
+            r.close()
+        finally:
+            os.chdir(cwd)
+    return dict(map=m, usn=usn, nn=nn, xs=xs, ys=ys)
+
+
+def upsample_case():
+    p = common.params()
+    with tempfile.TemporaryDirectory() as d:
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            xtg.write_view_file("view_info.txt", *common.views(p))
+            r = Reference(p)
+            a = np.random.default_rng(3).random((3, 5, 6)).astype(np.float32)
+            out = dict(inp=a, xy=r.upsample_xy(a), xyz=r.upsample_xyz(a))
+            r.close()
+        finally:
+            os.chdir(cwd)
+    return out
+
+
+def main():
+    if not ref_available():
+        sys.exit("oracle/_ref is not built (make -C oracle needs the reference tree)")
+    for name, (pk, vk, dk, iters) in CASES.items():
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **run_case(name, pk, vk, dk, iters))
+        print("wrote", name)
+    o64 = run_case("plain3d", *CASES["plain3d"], double=True)
+    np.savez_compressed(os.path.join(HERE, "plain3d_fp64.npz"), **o64)
+    np.savez_compressed(os.path.join(HERE, "rng_kat.npz"), table=rng_kat())
+    np.savez_compressed(os.path.join(HERE, "nhicd_select.npz"), **nhicd_case())
+    np.savez_compressed(os.path.join(HERE, "upsample.npz"), **upsample_case())
+    print("done")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1622 @@
+// xtg_api.cu -- libxtgpu: device buffers, the non-ICD kernels and the C ABI
+// declared in include/xtg.h.
+//
+// Kernels here (all HBM-bound integer/float streaming, no tensor cores):
+//   k_amatrix_batch   A-matrix columns (calcAMatrixColumnforAngle) for a list
+//   k_fp<MODE>        forward projection as a gather: one warp per (view, bin),
+//                     lanes over detector rows, candidate columns evaluated 32 at a
+//                     time and accumulated in the reference's (row, col) order
+//                     (FP32 = bit-exact with initErrorSinogam; FP64 = resync/cost)
+//   k_prior_cost64    qGGMRF prior over forward neighbour pairs, FP64
+//   k_running_cost64  data term from the running e, FP64
+//   k_zinger_refresh  ProjSelect = |e sqrt(w)| < T
+//   k_vsc_filter / k_radix_select / k_nhicd_compact   NHICD selection
+//   k_offset_* / k_var_*   offset d and variance re-estimation
+//   k_build_items / k_magsum / k_build_a16 / k_counts / object transposes
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/xtg.h"
+#include "xtg_internal.h"
+
+using namespace xtg;
+
+static thread_local char g_err[512];
+static void set_err(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      set_err("CUDA error %s at %s:%d: %s", cudaGetErrorName(e_), __FILE__, __LINE__,        \
+              cudaGetErrorString(e_));                                                       \
+      return XTG_E_CUDA;                                                                     \
+    }                                                                                        \
+  } while (0)
+
+#define NSLOT 64
+
+struct xtg_ctx {
+  xt_params prm;
+  xt_geom g;
+  xt_views v;
+  DevGeo G;
+  std::vector<float> hr;
+  std::vector<int> mcols, col_rank;
+  int n_masked = 0;
+  size_t ns = 0, nrt = 0, nvox = 0, nmag = 0, nxy = 0;
+  int vmax = 0;
+  // device arrays
+  float *d_y = nullptr, *d_w = nullptr, *d_e = nullptr, *d_d = nullptr, *d_x = nullptr, *d_mag = nullptr;
+  float *d_hr = nullptr, *d_cos = nullptr, *d_sin = nullptr, *d_ax = nullptr, *d_filt = nullptr, *d_tmp = nullptr;
+  float *d_num = nullptr, *d_den = nullptr, *d_thr = nullptr, *d_var = nullptr;
+  int *d_view_idx = nullptr, *d_view_start = nullptr, *d_view_num = nullptr, *d_fov = nullptr;
+  int *d_mcols = nullptr, *d_rank = nullptr, *d_counter = nullptr, *d_nhcnt = nullptr, *d_err = nullptr;
+  int *d_kth = nullptr;
+  int4 *d_items = nullptr, *d_nh = nullptr;
+  size_t items_cap = 0, nh_cap = 0;
+  double *d_red = nullptr;       // [8][NSLOT] reduction slots
+  double *d_absx = nullptr;      // [NSLOT]
+  unsigned long long *d_cnt = nullptr;  // [4]
+  uint4 *d_a16 = nullptr;
+  float *d_a16s = nullptr;
+  int a16_vmax = 0, a16_ok = 0;
+  // options
+  int a_mode = XTG_A_FP32, order = XTG_ORDER_PARALLEL, max_columns = 0;
+  unsigned long long seed = 0x5eed5eedULL;
+  int sm_count = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
+  int have_sino = 0;
+  long long launches = 0;
+  float last_kms = 0.f;
+  long long last_items = 0, last_rows = 0;
+  size_t dev_bytes = 0;
+  // Park-Miller state for the reference-order mode (randlib.c:119-168)
+  unsigned int sd[2] = {0, 0};
+  long rtmp = 0;
+};
+
+// ------------------------------------------------------------- helpers --
+template <typename T>
+static int dalloc(xtg_ctx *c, T **p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    set_err("cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    *p = nullptr;
+    return XTG_E_CUDA;
+  }
+  c->dev_bytes += n * sizeof(T);
+  return 0;
+}
+
+static unsigned blocks_for(size_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+static void rng_seed(xtg_ctx *c, unsigned int s) {
+  c->rtmp = s;
+  c->sd[0] = (unsigned)(c->rtmp >> 16);
+  c->sd[1] = (unsigned)(c->rtmp & 0xffff);
+}
+static double rng_next(xtg_ctx *c) {
+  c->sd[1] *= 16807u;
+  c->sd[0] *= 16807u;
+  c->rtmp = (long)((c->sd[0] >> 15) + ((c->sd[0] & 0x7fff) << 16));
+  c->rtmp += (long)c->sd[1];
+  if (c->rtmp & 0x80000000L) {
+    c->rtmp++;
+    c->rtmp &= 0x7fffffffL;
+  }
+  c->sd[0] = (unsigned)(c->rtmp >> 16);
+  c->sd[1] = (unsigned)(c->rtmp & 0xffff);
+  return ((double)c->rtmp) / 2147483647.0;
+}
+
+// ------------------------------------------------------------- kernels --
+__global__ void k_amatrix_batch(DevGeo G, const float *hr, const float *cosv, const float *sinv, int n,
+                                const int *rows, const int *cols, const int *views, float *vals, int *idx, int *cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = views[i];
+  float v[XT_AMAX];
+  int first;
+  const int m = xt_amatrix_view(G, hr + (size_t)p * XT_HR_STRIDE, cosv[p], sinv[p], rows[i], cols[i], v, &first);
+  // report the reference's (value, index) list: drop zero slots of the dense run
+  int k = 0;
+  for (int s = 0; s < m; s++)
+    if (v[s] > 0.f) {
+      vals[(size_t)i * G.amax + k] = v[s];
+      idx[(size_t)i * G.amax + k] = first + s;
+      k++;
+    }
+  cnt[i] = k;
+}
+
+struct FpArgs {
+  const float *x, *y, *d, *w, *hr, *cosv, *sinv;
+  const int *fov;
+  float *out;         // ax (MODE 0) or e (MODE 1, 2)
+  double *cost_slots; // MODE 2, 3
+  float T;
+  float delta;
+  double win_margin;
+};
+
+// MODE 0: out = A x (FP32); 1: out = e = y - A x - d (FP32);
+// 2: FP64 e64 = y - A x - d, out = (float)e64, data cost accumulated;
+// 3: FP64 data cost only.
+template <int MODE, int VF>
+__global__ void __launch_bounds__(256) k_fp(DevGeo G, FpArgs F) {
+  const int lane = threadIdx.x & 31;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  double cacc = 0.0;
+  if (gw < (long long)G.N_p * G.N_r) {
+    const int p = (int)(gw / G.N_r), r = (int)(gw % G.N_r), fr = F.fov[p];
+    const float cp = F.cosv[p], sp = F.sinv[p];
+    const float *H = F.hr + (size_t)p * XT_HR_STRIDE;
+    // columns whose footprint can reach bin r: R0 + r dr - dxy <= r_col < R0 + (r+1) dr + dxy
+    const double lo = (double)G.R0 + (double)r * G.delta_r - G.delta_xy - F.win_margin;
+    const double hi = (double)G.R0 + (double)(r + 1) * G.delta_r + G.delta_xy + F.win_margin;
+    for (int tb = 0; tb < G.N_t; tb += 32 * VF) {
+      float accf[VF];
+      double accd[VF];
+#pragma unroll
+      for (int c = 0; c < VF; c++) {
+        accf[c] = 0.f;
+        accd[c] = 0.0;
+      }
+      for (int j = 0; j < G.N_y; j++) {
+        const float yv = xt_coord(G.y0, j, G.delta_xy);
+        const double ys = (double)yv * (double)sp;
+        int klo, khi;
+        if (fabs((double)cp) < 1e-12) {
+          if (-ys >= lo && -ys <= hi) {
+            klo = 0;
+            khi = G.N_x - 1;
+          } else {
+            continue;
+          }
+        } else {
+          double xa = (lo + ys) / (double)cp, xb = (hi + ys) / (double)cp;
+          if (xa > xb) {
+            const double t = xa;
+            xa = xb;
+            xb = t;
+          }
+          const double ka = (xa - (double)G.x0) / (double)G.delta_xy - 0.5;
+          const double kb = (xb - (double)G.x0) / (double)G.delta_xy - 0.5;
+          if (kb < -4.0 || ka > (double)G.N_x + 4.0) continue;
+          klo = max(0, (int)floor(ka) - 2);
+          khi = min(G.N_x - 1, (int)ceil(kb) + 2);
+        }
+        for (int kb0 = klo; kb0 <= khi; kb0 += 32) {
+          const int k = kb0 + lane;
+          const float a = (k <= khi) ? xt_amatrix_entry(G, H, cp, sp, j, k, r) : 0.f;
+          unsigned m = __ballot_sync(0xffffffffu, a != 0.f);
+          while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const float aa = __shfl_sync(0xffffffffu, a, l);
+            const float *xp = F.x + (((size_t)fr * G.N_y + j) * G.N_x + (kb0 + l)) * G.N_z;
+#pragma unroll
+            for (int c = 0; c < VF; c++) {
+              const int t = tb + lane * VF + c;
+              if (t < G.N_t) {
+                const float xv = __ldg(xp + t / G.zovl);
+                if (MODE <= 1)
+                  accf[c] = __fadd_rn(accf[c], __fmul_rn(xv, aa));
+                else
+                  accd[c] += (double)xv * (double)aa;
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < VF; c++) {
+        const int t = tb + lane * VF + c;
+        if (t >= G.N_t) continue;
+        const size_t o = ((size_t)p * G.N_r + r) * G.N_t + t;
+        if (MODE == 0) {
+          F.out[o] = accf[c];
+        } else if (MODE == 1) {
+          F.out[o] = __fsub_rn(__fsub_rn(F.y[o], accf[c]), F.d[(size_t)r * G.N_t + t]);
+        } else {
+          const double e64 = (double)F.y[o] - accd[c] - (double)F.d[(size_t)r * G.N_t + t];
+          if (MODE == 2) F.out[o] = (float)e64;
+          const double w64 = (double)F.w[o];
+          const double s = e64 * sqrt(w64);
+          if (fabs(s) < (double)F.T)
+            cacc += s * s;
+          else
+            cacc += 2.0 * (double)F.delta * (double)F.T * fabs(s) + (double)F.T * (double)F.T * (1.0 - 2.0 * (double)F.delta);
+        }
+      }
+    }
+  }
+  if (MODE >= 2) {
+    __shared__ double red[8];
+    for (int off = 16; off > 0; off >>= 1) cacc += __shfl_xor_sync(0xffffffffu, cacc, off);
+    if (lane == 0) red[threadIdx.x >> 5] = cacc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += red[q];
+      atomicAdd(&F.cost_slots[blockIdx.x % NSLOT], s);
+    }
+  }
+}
+
+// qGGMRF prior over forward neighbour pairs (XT_ICD_update.c:202-294), FP64.
+__global__ void k_prior_cost64(DevGeo G, const float *x, double *slots) {
+  const size_t n = (size_t)G.N_time * G.N_y * G.N_x * G.N_z;
+  double acc = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i % G.N_z);
+    size_t r = i / G.N_z;
+    const int k = (int)(r % G.N_x);
+    r /= G.N_x;
+    const int j = (int)(r % G.N_y);
+    const int f = (int)(r / G.N_y);
+    const double v = x[i];
+    const double sq = G.Sigma_S_Q, sqp = G.Sigma_S_Q_P, cs = G.C_S, pp = G.MRF_P;
+    auto X = [&](int ff, int jj, int kk, int zz) -> double {
+      return (double)x[(((size_t)ff * G.N_y + jj) * G.N_x + kk) * G.N_z + zz];
+    };
+    auto term = [&](int dz, int dy, int dx) {
+      const int jj = j + dy, kk = k + dx, zz = z + dz;
+      if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x || zz >= G.N_z) return;
+      acc += (double)G.SF[(1 + dz) * 9 + (1 + dy) * 3 + (1 + dx)] * xt_qggmrf_value64(v - X(f, jj, kk, zz), sq, sqp, cs, pp);
+    };
+    term(0, 0, 1);
+    term(0, 1, -1);
+    term(0, 1, 0);
+    term(0, 1, 1);
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) term(1, dy, dx);
+    if (f + 1 < G.N_time)
+      acc += (double)G.TF * xt_qggmrf_value64(v - X(f + 1, j, k, z), G.Sigma_T_Q, G.Sigma_T_Q_P, G.C_T, pp);
+  }
+  __shared__ double red[32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += red[q];
+    atomicAdd(&slots[blockIdx.x % NSLOT], s);
+  }
+}
+
+// data term from the running e (XT_ICD_update.c:188-200), FP64 arithmetic.
+__global__ void k_running_cost64(size_t n, const float *e, const float *w, float T, float delta, double *slots) {
+  double acc = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double s = (double)e[i] * sqrt((double)w[i]);
+    if (fabs(s) < (double)T)
+      acc += s * s;
+    else
+      acc += 2.0 * (double)delta * (double)T * fabs(s) + (double)T * (double)T * (1.0 - 2.0 * (double)delta);
+  }
+  __shared__ double red[32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += red[q];
+    atomicAdd(&slots[blockIdx.x % NSLOT], s);
+  }
+}
+
+// ProjSelect = |e sqrt(w)| < T, in double like the reference's mixed expression.
+__global__ void k_zinger_refresh(size_t n, const float *e, const float *w, float T, unsigned char *sel,
+                                 unsigned long long *count) {
+  unsigned c = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const unsigned char s = (fabs((double)e[i] * sqrt((double)w[i])) < (double)T) ? 1 : 0;
+    if (sel) sel[i] = s;
+    c += s;
+  }
+  for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// ComputeVSC (XT_NHICD.c:128-162): 5x5 Hamming-weighted sum, summed in the
+// reference's order in FP32.
+__constant__ float c_vsc[25] = {0.0064f, 0.0432f, 0.0800f, 0.0432f, 0.0064f, 0.0432f, 0.2916f, 0.5400f, 0.2916f,
+                                0.0432f, 0.0800f, 0.5400f, 1.0000f, 0.5400f, 0.0800f, 0.0432f, 0.2916f, 0.5400f,
+                                0.2916f, 0.0432f, 0.0064f, 0.0432f, 0.0800f, 0.0432f, 0.0064f};
+
+__global__ void k_vsc_filter(int nseg, int ny, int nx, const float *map, float *out) {
+  const size_t n = (size_t)nseg * ny * nx;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(q % nx);
+    const int j = (int)((q / nx) % ny);
+    const size_t seg = q / ((size_t)nx * ny);
+    const float *m = map + seg * (size_t)nx * ny;
+    float f = 0.f;
+    for (int p = -2; p <= 2; p++)
+      for (int s = -2; s <= 2; s++)
+        if (j + p >= 0 && j + p < ny && k + s >= 0 && k + s < nx)
+          f = __fadd_rn(f, __fmul_rn(c_vsc[(p + 2) * 5 + s + 2], m[(size_t)(j + p) * nx + (k + s)]));
+    out[q] = f;
+  }
+}
+
+// k-th smallest (1-based) of each segment by 4 passes of 8-bit radix
+// histograms; the exact order statistic RandomizedSelect returns
+// (XT_NHICD.c:63-126).
+__global__ void __launch_bounds__(1024) k_radix_select(const float *vals, int seglen, const int *kth, float *out) {
+  __shared__ unsigned hist[256];
+  __shared__ unsigned s_prefix, s_mask, s_k;
+  const float *v = vals + (size_t)blockIdx.x * seglen;
+  if (threadIdx.x == 0) {
+    s_prefix = 0;
+    s_mask = 0;
+    s_k = (unsigned)kth[blockIdx.x];
+  }
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    const unsigned pre = s_prefix, msk = s_mask;
+    for (int i = threadIdx.x; i < seglen; i += blockDim.x) {
+      const unsigned key = xt_f2key(v[i]);
+      if ((key & msk) == pre) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned k = s_k, cum = 0;
+      int b = 0;
+      for (; b < 255; b++) {
+        if (cum + hist[b] >= k) break;
+        cum += hist[b];
+      }
+      s_k = k - cum;
+      s_prefix = pre | ((unsigned)b << shift);
+      s_mask = msk | (255u << shift);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = xt_key2f(s_prefix);
+}
+
+// columns above the threshold -> NHICD work items.  List 0 holds the
+// (frame, block) pairs the reference updates in its first half-pass (block
+// parity = frame parity, XT_ICD_update.c:846-857), list 1 the others.
+__global__ void k_nhicd_compact(int ntime, int nzb, int ny, int nx, const float *filt, const float *thr, int4 *list0,
+                                int4 *list1, int *cnt, int cap0, int cap1) {
+  const size_t n = (size_t)ntime * nzb * ny * nx;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t seg = q / ((size_t)nx * ny);
+    if (!(filt[q] > thr[seg])) continue;
+    const int k = (int)(q % nx), j = (int)((q / nx) % ny);
+    const int b = (int)(seg % nzb), f = (int)(seg / nzb);
+    const int h = ((f & 1) == (b & 1)) ? 0 : 1;
+    const int slot = atomicAdd(&cnt[h], 1);
+    if (h == 0) {
+      if (slot < cap0) list0[slot] = make_int4(f, j, k, b);
+    } else {
+      if (slot < cap1) list1[slot] = make_int4(f, j, k, b);
+    }
+  }
+}
+
+__global__ void k_clamp_count(int *cnt, int cap0, int cap1) {
+  if (threadIdx.x == 0) {
+    cnt[0] = min(cnt[0], cap0);
+    cnt[1] = min(cnt[1], cap1);
+  }
+}
+
+// update_Sinogram_Offset (XT_ICD_update.c:666-759), one thread per (r, t),
+// views summed in order; FP32 like the reference, sums for gamma in FP64.
+__global__ void k_offset_numden(DevGeo G, const float *e, const float *w, const float *d, float *num, float *den,
+                                double *sums) {
+  const int nrt = G.N_r * G.N_t;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  double a = 0, b = 0;
+  if (q < nrt) {
+    float nm = 0.f, dn = 0.f;
+    const float td = G.T * G.delta;
+    for (int p = 0; p < G.N_p; p++) {
+      const size_t s = (size_t)p * nrt + q;
+      const float ev = e[s], wv = w[s];
+      const float temp = (float)((double)td * sqrt((double)wv));
+      if (fabs((double)ev * sqrt((double)wv)) < (double)G.T) {
+        nm = __fadd_rn(nm, __fmul_rn(ev, wv));
+        dn = __fadd_rn(dn, wv);
+      } else {
+        const float sign = (float)((ev > 0.f) - (ev < 0.f));
+        nm = __fadd_rn(nm, __fmul_rn(temp, sign));
+        dn = (float)((double)dn + (double)temp / fabs((double)ev));
+      }
+    }
+    num[q] = nm;
+    den[q] = dn;
+    a = (double)d[q] + (double)nm / (double)dn;
+    b = 1.0 / (double)dn;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, off);
+    b += __shfl_xor_sync(0xffffffffu, b, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&sums[0], a);
+    atomicAdd(&sums[1], b);
+  }
+}
+
+__global__ void k_offset_apply(DevGeo G, float *e, float *d, const float *num, const float *den, const double *sums,
+                               int zero_mean) {
+  const int nrt = G.N_r * G.N_t;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrt) return;
+  const float gamma = zero_mean ? (float)(sums[0] / sums[1]) : 0.f;
+  const float corr = __fdiv_rn(__fsub_rn(num[q], gamma), den[q]);
+  d[q] = __fadd_rn(d[q], corr);
+  for (int p = 0; p < G.N_p; p++) {
+    const size_t s = (size_t)p * nrt + q;
+    e[s] = __fsub_rn(e[s], corr);
+  }
+}
+
+// update_variance_parameter (XT_ICD_update.c:633-664): w *= var, sum the
+// data term (the zinger branch uses sqrt(w * var) after that product, as the
+// reference does), then var = sum / N and w /= var.
+__global__ void k_var_sum(size_t n, const float *e, float *w, const float *var, float T, float delta, double *slots) {
+  double acc = 0.0;
+  const float vv = *var;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float w0 = w[i];
+    const bool sel = fabs((double)e[i] * sqrt((double)w0)) < (double)T;
+    const float w1 = __fmul_rn(w0, vv);
+    w[i] = w1;
+    if (sel)
+      acc += (double)__fmul_rn(__fmul_rn(e[i], e[i]), w1);
+    else
+      acc += fabs((double)e[i]) * (double)delta * (double)T * sqrt((double)__fmul_rn(w1, vv));
+  }
+  __shared__ double red[32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += red[q];
+    atomicAdd(&slots[blockIdx.x % NSLOT], s);
+  }
+}
+
+__global__ void k_var_finish(const double *slots, double n, float *var) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < NSLOT; q++) s += slots[q];
+    *var = (float)(s / n);
+  }
+}
+
+__global__ void k_scale_weights(size_t n, float *w, const float *var) {
+  const float vv = *var;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    w[i] = __fdiv_rn(w[i], vv);
+}
+
+// [N_time][N_z][N_y][N_x] <-> [N_time][N_y][N_x][N_z]
+__global__ void k_obj_h2d(DevGeo G, const float *src, float *dst) {
+  const size_t n = (size_t)G.N_time * G.N_z * G.N_y * G.N_x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i % G.N_x);
+    size_t r = i / G.N_x;
+    const int j = (int)(r % G.N_y);
+    r /= G.N_y;
+    const int z = (int)(r % G.N_z);
+    const size_t f = r / G.N_z;
+    dst[((f * G.N_y + j) * G.N_x + k) * G.N_z + z] = src[i];
+  }
+}
+__global__ void k_obj_d2h(DevGeo G, const float *src, float *dst) {
+  const size_t n = (size_t)G.N_time * G.N_z * G.N_y * G.N_x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i % G.N_x);
+    size_t r = i / G.N_x;
+    const int j = (int)(r % G.N_y);
+    r /= G.N_y;
+    const int z = (int)(r % G.N_z);
+    const size_t f = r / G.N_z;
+    dst[i] = src[((f * G.N_y + j) * G.N_x + k) * G.N_z + z];
+  }
+}
+
+// random visiting order of every (frame, masked column) whole z-line
+__global__ void k_build_items(int n, int n_masked, int nx, const int *mcols, unsigned long long key, int4 *items) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int v = (int)xt_perm((uint32_t)q, (uint32_t)n, key);
+  const int f = v / n_masked, c = mcols[v % n_masked];
+  items[q] = make_int4(f, c / nx, c % nx, -1);
+}
+
+// sum of MagUpdateMap over the random lists (XT_ICD_update.c:889-894)
+__global__ void k_magsum(DevGeo G, int n_masked, const int *mcols, const float *mag, double *slots) {
+  const size_t n = (size_t)G.N_time * G.nzb * n_masked;
+  double acc = 0;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t seg = q / n_masked;
+    acc += (double)mag[seg * (size_t)G.N_y * G.N_x + mcols[q % n_masked]];
+  }
+  __shared__ double red[32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += red[q];
+    atomicAdd(&slots[blockIdx.x % NSLOT], s);
+  }
+}
+
+// FP16 A records: per (frame, masked column, view) one uint4 =
+// {first | n << 16, half2(v0, v1), half2(v2, v3), 0}, values (A * delta_t)
+// divided by the column's largest value, which is kept in FP32.
+__global__ void k_build_a16(DevGeo G, const float *hr, const float *cosv, const float *sinv, const int *view_idx,
+                            const int *view_start, const int *view_num, int n_masked, const int *mcols, int vmax,
+                            uint4 *rec, float *scale) {
+  const int lane = threadIdx.x & 31;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (gw >= (long long)G.N_time * n_masked) return;
+  const int f = (int)(gw / n_masked), ci = (int)(gw % n_masked);
+  const int c = mcols[ci], row = c / G.N_x, col = c % G.N_x;
+  const int V = view_num[f], vs = view_start[f];
+  float mx = 0.f;
+  for (int v = lane; v < V; v += 32) {
+    const int p = view_idx[vs + v];
+    float vals[XT_AMAX];
+    int first;
+    const int n = xt_amatrix_view(G, hr + (size_t)p * XT_HR_STRIDE, cosv[p], sinv[p], row, col, vals, &first);
+    for (int s = 0; s < n; s++) mx = fmaxf(mx, __fmul_rn(vals[s], G.delta_t));
+  }
+  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  const float sc = mx > 0.f ? mx : 1.f;
+  if (lane == 0) scale[gw] = sc;
+  for (int v = lane; v < V; v += 32) {
+    const int p = view_idx[vs + v];
+    float vals[XT_AMAX];
+    int first;
+    int n = xt_amatrix_view(G, hr + (size_t)p * XT_HR_STRIDE, cosv[p], sinv[p], row, col, vals, &first);
+    n = min(n, 4);
+    float q[4];
+    for (int s = 0; s < 4; s++) q[s] = (s < n) ? __fmul_rn(vals[s], G.delta_t) / sc : 0.f;
+    const __half2 h01 = __floats2half2_rn(q[0], q[1]);
+    const __half2 h23 = __floats2half2_rn(q[2], q[3]);
+    uint4 r4;
+    r4.x = (unsigned)(first & 0xffff) | ((unsigned)n << 16);
+    r4.y = *reinterpret_cast<const unsigned *>(&h01);
+    r4.z = *reinterpret_cast<const unsigned *>(&h23);
+    r4.w = 0u;
+    rec[(size_t)gw * vmax + v] = r4;
+  }
+}
+
+// genSinogram_subsampleCounts (XT_genSinogram.c:303-374)
+__global__ void k_counts(DevGeo G, int mxy, int mz, const float *bright, const float *counts, float bh, float *y,
+                         float *w) {
+  const size_t n = (size_t)G.N_p * G.N_r * G.N_t;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int t = (int)(q % G.N_t);
+    const int r = (int)((q / G.N_t) % G.N_r);
+    const size_t p = q / ((size_t)G.N_t * G.N_r);
+    const int Rr = G.N_r * mxy, Tt = G.N_t * mz;
+    float wt = 0.f, bt = 0.f;
+    for (int a = 0; a < mxy; a++)
+      for (int b = 0; b < mz; b++) {
+        wt = __fadd_rn(wt, counts[(p * Rr + (size_t)(r * mxy + a)) * Tt + (t * mz + b)]);
+        bt = __fadd_rn(bt, bright[(size_t)(r * mxy + a) * Tt + (t * mz + b)]);
+      }
+    const float tmp = (float)log((double)__fdiv_rn(bt, wt));
+    y[q] = (float)((double)bh * tmp * tmp + tmp);
+    w[q] = wt;
+  }
+}
+
+__global__ void k_fill(size_t n, float *p, float v) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+// ------------------------------------------------------------ host side --
+static DevGeo make_devgeo(const xt_geom &g, int positivity) {
+  DevGeo G;
+  memset(&G, 0, sizeof(G));
+  G.N_r = g.N_r; G.N_t = g.N_t; G.N_p = g.N_p; G.N_x = g.N_x; G.N_y = g.N_y; G.N_z = g.N_z;
+  G.N_time = g.N_time; G.zovl = g.zovl; G.nzb = g.nzb; G.zstep = g.zstep; G.amax = g.amax;
+  G.positivity = positivity;
+  G.delta_r = g.delta_r; G.delta_t = g.delta_t; G.R0 = g.R0; G.RMax = g.RMax; G.x0 = g.x0; G.y0 = g.y0;
+  G.delta_xy = g.delta_xy; G.OffsetR = g.OffsetR; G.MRF_P = g.MRF_P; G.C_S = g.C_S; G.C_T = g.C_T;
+  G.alpha = g.alpha; G.Sigma_S_Q = g.Sigma_S_Q; G.Sigma_S_Q_P = g.Sigma_S_Q_P; G.Sigma_T_Q = g.Sigma_T_Q;
+  G.Sigma_T_Q_P = g.Sigma_T_Q_P;
+  for (int i = 0; i < 27; i++) G.SF[i] = g.SF[i];
+  G.TF = g.TF; G.T = g.T; G.delta = g.delta;
+  return G;
+}
+
+template <int MODE>
+static cudaError_t launch_fp(xtg_ctx *c, float *out, double *slots) {
+  FpArgs F;
+  F.x = c->d_x; F.y = c->d_y; F.d = c->d_d; F.w = c->d_w; F.hr = c->d_hr; F.cosv = c->d_cos; F.sinv = c->d_sin;
+  F.fov = c->d_fov; F.out = out; F.cost_slots = slots; F.T = c->g.T; F.delta = c->g.delta;
+  F.win_margin = 1e-4 * (double)c->g.N_r * c->g.delta_r + 1e-3 * c->g.delta_r;
+  const long long warps = (long long)c->g.N_p * c->g.N_r;
+  const unsigned grid = (unsigned)((warps + 7) / 8);
+  const int vf = std::min(4, std::max(1, (c->g.N_t + 31) / 32));
+  if (vf == 1)
+    k_fp<MODE, 1><<<grid, 256, 0, c->st>>>(c->G, F);
+  else if (vf == 2)
+    k_fp<MODE, 2><<<grid, 256, 0, c->st>>>(c->G, F);
+  else
+    k_fp<MODE, 4><<<grid, 256, 0, c->st>>>(c->G, F);
+  c->launches++;
+  return cudaGetLastError();
+}
+
+extern "C" {
+
+const char *xtg_last_error(void) { return g_err; }
+int xtg_abi_version(void) { return XTG_ABI_VERSION; }
+
+void xtg_destroy(xtg_ctx *c) {
+  if (!c) return;
+  void *ptrs[] = {c->d_y, c->d_w, c->d_e, c->d_d, c->d_x, c->d_mag, c->d_hr, c->d_cos, c->d_sin, c->d_ax,
+                  c->d_filt, c->d_tmp, c->d_num, c->d_den, c->d_thr, c->d_var, c->d_view_idx, c->d_view_start,
+                  c->d_view_num, c->d_fov, c->d_mcols, c->d_rank, c->d_counter, c->d_nhcnt, c->d_err, c->d_kth,
+                  c->d_items, c->d_nh, c->d_red, c->d_absx, c->d_cnt, c->d_a16, c->d_a16s};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ek0) cudaEventDestroy(c->ek0);
+  if (c->ek1) cudaEventDestroy(c->ek1);
+  if (c->st) cudaStreamDestroy(c->st);
+  xt_views_free(&c->v);
+  delete c;
+}
+
+int xtg_create(const xt_params *prm, const double *times, const double *angles, int32_t n, xtg_ctx **out) {
+  *out = nullptr;
+  if (!prm || !times || !angles || !out) {
+    set_err("xtg_create: null argument");
+    return XTG_E_ARG;
+  }
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || ndev == 0) {
+    set_err("xtg_create: no CUDA device (%s); this library has no CPU path", cudaGetErrorString(ce));
+    return XTG_E_CUDA;
+  }
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) {
+    set_err("xtg_create: device %s is sm_%d%d; libxtgpu is built for sm_100a", prop.name, prop.major, prop.minor);
+    return XTG_E_CUDA;
+  }
+  xtg_ctx *c = new xtg_ctx();
+  c->prm = *prm;
+  char err[512];
+  if (xt_geom_derive(prm, &c->g, err, sizeof(err)) != 0) {
+    set_err("%s", err);
+    delete c;
+    return XTG_E_ARG;
+  }
+  if (xt_views_build(&c->g, times, angles, n, &c->v, err, sizeof(err)) != 0) {
+    set_err("%s", err);
+    xtg_destroy(c);
+    return XTG_E_ARG;
+  }
+  const xt_geom &g = c->g;
+  c->G = make_devgeo(g, prm->positivity);
+  c->sm_count = prop.multiProcessorCount;
+  c->ns = (size_t)g.N_p * g.N_r * g.N_t;
+  c->nrt = (size_t)g.N_r * g.N_t;
+  c->nxy = (size_t)g.N_x * g.N_y;
+  c->nvox = (size_t)g.N_time * g.N_z * c->nxy;
+  c->nmag = (size_t)g.N_time * g.nzb * c->nxy;
+  c->hr.resize((size_t)g.N_p * XT_HR_STRIDE);
+  xt_detector_response(&g, &c->v, c->hr.data());
+  c->col_rank.assign(c->nxy, -1);
+  for (int j = 0; j < g.N_y; j++)
+    for (int k = 0; k < g.N_x; k++)
+      if (xt_in_mask(&g, j, k)) {
+        c->col_rank[(size_t)j * g.N_x + k] = (int)c->mcols.size();
+        c->mcols.push_back(j * g.N_x + k);
+      }
+  c->n_masked = (int)c->mcols.size();
+  for (int f = 0; f < g.N_time; f++) c->vmax = std::max(c->vmax, c->v.view_num[f]);
+  rng_seed(c, 761521u);  // the reference seeds once in main (XT_Engine.c:137)
+
+  int rc = 0;
+  rc |= dalloc(c, &c->d_y, c->ns);
+  rc |= dalloc(c, &c->d_w, c->ns);
+  rc |= dalloc(c, &c->d_e, c->ns);
+  rc |= dalloc(c, &c->d_d, c->nrt);
+  rc |= dalloc(c, &c->d_x, c->nvox);
+  rc |= dalloc(c, &c->d_mag, c->nmag);
+  rc |= dalloc(c, &c->d_filt, c->nmag);
+  rc |= dalloc(c, &c->d_hr, c->hr.size());
+  rc |= dalloc(c, &c->d_cos, (size_t)g.N_p);
+  rc |= dalloc(c, &c->d_sin, (size_t)g.N_p);
+  rc |= dalloc(c, &c->d_num, c->nrt);
+  rc |= dalloc(c, &c->d_den, c->nrt);
+  rc |= dalloc(c, &c->d_thr, (size_t)g.N_time * g.nzb);
+  rc |= dalloc(c, &c->d_kth, (size_t)g.N_time * g.nzb);
+  rc |= dalloc(c, &c->d_var, 1);
+  rc |= dalloc(c, &c->d_view_idx, (size_t)g.N_p);
+  rc |= dalloc(c, &c->d_view_start, (size_t)g.N_time);
+  rc |= dalloc(c, &c->d_view_num, (size_t)g.N_time);
+  rc |= dalloc(c, &c->d_fov, (size_t)g.N_p);
+  rc |= dalloc(c, &c->d_mcols, (size_t)c->n_masked);
+  rc |= dalloc(c, &c->d_rank, c->nxy);
+  rc |= dalloc(c, &c->d_counter, 8);
+  rc |= dalloc(c, &c->d_nhcnt, 2);
+  rc |= dalloc(c, &c->d_err, 1);
+  rc |= dalloc(c, &c->d_red, 8 * NSLOT);
+  rc |= dalloc(c, &c->d_absx, NSLOT);
+  rc |= dalloc(c, &c->d_cnt, 4);
+  c->items_cap = (size_t)g.N_time * c->n_masked + 1;
+  rc |= dalloc(c, &c->d_items, c->items_cap);
+  c->nh_cap = (size_t)g.N_time * g.nzb * (c->n_masked / XT_NHICD_CHUNKS + 1) + 2;
+  rc |= dalloc(c, &c->d_nh, c->nh_cap);
+  if (rc) {
+    xtg_destroy(c);
+    return XTG_E_CUDA;
+  }
+  CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&c->ev0));
+  CK(cudaEventCreate(&c->ev1));
+  CK(cudaEventCreate(&c->ek0));
+  CK(cudaEventCreate(&c->ek1));
+  CK(cudaMemcpy(c->d_hr, c->hr.data(), c->hr.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_cos, c->v.cosv, (size_t)g.N_p * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_sin, c->v.sinv, (size_t)g.N_p * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_view_idx, c->v.view_idx, (size_t)g.N_p * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_view_start, c->v.view_start, (size_t)g.N_time * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_view_num, c->v.view_num, (size_t)g.N_time * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_fov, c->v.frame_of_view, (size_t)g.N_p * 4, cudaMemcpyHostToDevice));
+  if (c->n_masked) CK(cudaMemcpy(c->d_mcols, c->mcols.data(), (size_t)c->n_masked * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_rank, c->col_rank.data(), c->nxy * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemset(c->d_x, 0, c->nvox * 4));
+  CK(cudaMemset(c->d_e, 0, c->ns * 4));
+  CK(cudaMemset(c->d_d, 0, c->nrt * 4));
+  CK(cudaMemset(c->d_mag, 0, c->nmag * 4));
+  CK(cudaMemset(c->d_err, 0, 4));
+  const float var = g.var_est;
+  CK(cudaMemcpy(c->d_var, &var, 4, cudaMemcpyHostToDevice));
+  *out = c;
+  return XTG_OK;
+}
+
+int xtg_dims(const xtg_ctx *c, int32_t *d) {
+  if (!c || !d) return XTG_E_ARG;
+  const xt_geom &g = c->g;
+  d[0] = g.N_x; d[1] = g.N_y; d[2] = g.N_z; d[3] = g.N_time; d[4] = g.N_r; d[5] = g.N_t; d[6] = g.N_p;
+  d[7] = g.nzb; d[8] = g.zovl; d[9] = g.amax;
+  return 0;
+}
+
+int xtg_geometry(const xtg_ctx *c, xt_geom *g) {
+  if (!c || !g) return XTG_E_ARG;
+  *g = c->g;
+  return 0;
+}
+
+int xtg_get_hr(const xtg_ctx *c, float *hr) {
+  if (!c || !hr) return XTG_E_ARG;
+  memcpy(hr, c->hr.data(), c->hr.size() * 4);
+  return 0;
+}
+
+int xtg_set_options(xtg_ctx *c, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed) {
+  if (!c || (a_mode != XTG_A_FP32 && a_mode != XTG_A_FP16) ||
+      (order != XTG_ORDER_PARALLEL && order != XTG_ORDER_SEQUENTIAL) || max_columns < 0) {
+    set_err("xtg_set_options: bad option");
+    return XTG_E_ARG;
+  }
+  if (a_mode == XTG_A_FP16 && (int)ceil(2.0 * c->g.delta_xy / c->g.delta_r) + 1 > 4) {
+    set_err("xtg_set_options: FP16 A supports delta_xy <= 1.5 detector bins");
+    return XTG_E_ARG;
+  }
+  c->a_mode = a_mode;
+  c->order = order;
+  c->max_columns = max_columns;
+  c->seed = seed;
+  return 0;
+}
+
+static int check_err_flag(xtg_ctx *c) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->d_err, 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (h) {
+    CK(cudaMemsetAsync(c->d_err, 0, 4, c->st));
+    set_err("non-finite voxel value in an update (theta2 + prior weight <= 0)");
+    return XTG_E_NUMERIC;
+  }
+  return 0;
+}
+
+int xtg_upload_sino(xtg_ctx *c, const float *y, const float *w, const float *d) {
+  if (!c || !y || !w) {
+    set_err("xtg_upload_sino: null argument");
+    return XTG_E_ARG;
+  }
+  CK(cudaMemcpyAsync(c->d_y, y, c->ns * 4, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_w, w, c->ns * 4, cudaMemcpyHostToDevice, c->st));
+  if (d)
+    CK(cudaMemcpyAsync(c->d_d, d, c->nrt * 4, cudaMemcpyHostToDevice, c->st));
+  else
+    CK(cudaMemsetAsync(c->d_d, 0, c->nrt * 4, c->st));
+  k_scale_weights<<<std::min<unsigned>(blocks_for(c->ns, 256), 4096), 256, 0, c->st>>>(c->ns, c->d_w, c->d_var);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  c->have_sino = 1;
+  return 0;
+}
+
+int xtg_upload_counts(xtg_ctx *c, const float *bright, const float *counts, double bh, const float *d) {
+  if (!c || !bright || !counts) return XTG_E_ARG;
+  if (c->prm.sinobin != 3) {
+    set_err("xtg_upload_counts: the context was not created with sinobin = 3");
+    return XTG_E_STATE;
+  }
+  const int mxy = (int)c->g.mult_xy, mz = (int)c->g.mult_z;
+  const size_t nb = (size_t)c->g.N_r * mxy * c->g.N_t * mz, nc = nb * c->g.N_p;
+  float *db = nullptr, *dc = nullptr;
+  CK(cudaMalloc(&db, nb * 4));
+  if (cudaMalloc(&dc, nc * 4) != cudaSuccess) {
+    cudaFree(db);
+    set_err("xtg_upload_counts: out of device memory");
+    return XTG_E_CUDA;
+  }
+  cudaMemcpyAsync(db, bright, nb * 4, cudaMemcpyHostToDevice, c->st);
+  cudaMemcpyAsync(dc, counts, nc * 4, cudaMemcpyHostToDevice, c->st);
+  k_counts<<<std::min<unsigned>(blocks_for(c->ns, 256), 8192), 256, 0, c->st>>>(c->G, mxy, mz, db, dc, (float)bh,
+                                                                               c->d_y, c->d_w);
+  k_scale_weights<<<std::min<unsigned>(blocks_for(c->ns, 256), 4096), 256, 0, c->st>>>(c->ns, c->d_w, c->d_var);
+  c->launches += 2;
+  if (d)
+    cudaMemcpyAsync(c->d_d, d, c->nrt * 4, cudaMemcpyHostToDevice, c->st);
+  else
+    cudaMemsetAsync(c->d_d, 0, c->nrt * 4, c->st);
+  cudaError_t e = cudaStreamSynchronize(c->st);
+  cudaFree(db);
+  cudaFree(dc);
+  CK(e);
+  c->have_sino = 1;
+  return 0;
+}
+
+int xtg_upload_object(xtg_ctx *c, const float *x) {
+  if (!c || !x) return XTG_E_ARG;
+  if (!c->d_tmp && dalloc(c, &c->d_tmp, c->nvox)) return XTG_E_CUDA;
+  CK(cudaMemcpyAsync(c->d_tmp, x, c->nvox * 4, cudaMemcpyHostToDevice, c->st));
+  k_obj_h2d<<<std::min<unsigned>(blocks_for(c->nvox, 256), 8192), 256, 0, c->st>>>(c->G, c->d_tmp, c->d_x);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int xtg_download_object(xtg_ctx *c, float *x) {
+  if (!c || !x) return XTG_E_ARG;
+  if (!c->d_tmp && dalloc(c, &c->d_tmp, c->nvox)) return XTG_E_CUDA;
+  k_obj_d2h<<<std::min<unsigned>(blocks_for(c->nvox, 256), 8192), 256, 0, c->st>>>(c->G, c->d_x, c->d_tmp);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(x, c->d_tmp, c->nvox * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+#define XTG_COPY_FN(name, dev, count, kind, ptype)                        \
+  int name(xtg_ctx *c, ptype p) {                                         \
+    if (!c || !p) return XTG_E_ARG;                                       \
+    CK(cudaMemcpyAsync((void *)(kind == cudaMemcpyDeviceToHost ? (void *)p : (void *)c->dev), \
+                       (const void *)(kind == cudaMemcpyDeviceToHost ? (const void *)c->dev : (const void *)p), \
+                       (count) * 4, kind, c->st));                        \
+    CK(cudaStreamSynchronize(c->st));                                     \
+    return 0;                                                             \
+  }
+XTG_COPY_FN(xtg_get_error_sino, d_e, c->ns, cudaMemcpyDeviceToHost, float *)
+XTG_COPY_FN(xtg_set_error_sino, d_e, c->ns, cudaMemcpyHostToDevice, const float *)
+XTG_COPY_FN(xtg_get_weight, d_w, c->ns, cudaMemcpyDeviceToHost, float *)
+XTG_COPY_FN(xtg_get_offset, d_d, c->nrt, cudaMemcpyDeviceToHost, float *)
+XTG_COPY_FN(xtg_set_offset, d_d, c->nrt, cudaMemcpyHostToDevice, const float *)
+XTG_COPY_FN(xtg_get_magmap, d_mag, c->nmag, cudaMemcpyDeviceToHost, float *)
+XTG_COPY_FN(xtg_set_magmap, d_mag, c->nmag, cudaMemcpyHostToDevice, const float *)
+
+int xtg_get_variance(xtg_ctx *c, double *v) {
+  if (!c || !v) return XTG_E_ARG;
+  float h = 0;
+  CK(cudaMemcpyAsync(&h, c->d_var, 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *v = h;
+  return 0;
+}
+
+int xtg_set_variance(xtg_ctx *c, double v) {
+  if (!c || !(v > 0)) return XTG_E_ARG;
+  const float h = (float)v;
+  CK(cudaMemcpyAsync(c->d_var, &h, 4, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int xtg_amatrix(xtg_ctx *c, int32_t n, const int32_t *rows, const int32_t *cols, const int32_t *views, float *vals,
+                int32_t *idx, int32_t *cnt) {
+  if (!c || n < 0 || (n && (!rows || !cols || !views || !vals || !idx || !cnt))) return XTG_E_ARG;
+  if (n == 0) return 0;
+  for (int i = 0; i < n; i++)
+    if (rows[i] < 0 || rows[i] >= c->g.N_y || cols[i] < 0 || cols[i] >= c->g.N_x || views[i] < 0 ||
+        views[i] >= c->g.N_p) {
+      set_err("xtg_amatrix: triple %d out of range", i);
+      return XTG_E_ARG;
+    }
+  int *dr, *dcol, *dv, *di, *dc;
+  float *dval;
+  const size_t na = (size_t)n * c->g.amax;
+  CK(cudaMalloc(&dr, (size_t)n * 4 * 3 + (size_t)n * 4 + na * 8));
+  dcol = dr + n;
+  dv = dcol + n;
+  dc = dv + n;
+  dval = reinterpret_cast<float *>(dc + n);
+  di = reinterpret_cast<int *>(dval + na);
+  cudaMemcpyAsync(dr, rows, (size_t)n * 4, cudaMemcpyHostToDevice, c->st);
+  cudaMemcpyAsync(dcol, cols, (size_t)n * 4, cudaMemcpyHostToDevice, c->st);
+  cudaMemcpyAsync(dv, views, (size_t)n * 4, cudaMemcpyHostToDevice, c->st);
+  k_amatrix_batch<<<blocks_for(n, 128), 128, 0, c->st>>>(c->G, c->d_hr, c->d_cos, c->d_sin, n, dr, dcol, dv, dval, di, dc);
+  c->launches++;
+  cudaMemcpyAsync(vals, dval, na * 4, cudaMemcpyDeviceToHost, c->st);
+  cudaMemcpyAsync(idx, di, na * 4, cudaMemcpyDeviceToHost, c->st);
+  cudaMemcpyAsync(cnt, dc, (size_t)n * 4, cudaMemcpyDeviceToHost, c->st);
+  cudaError_t e = cudaStreamSynchronize(c->st);
+  cudaFree(dr);
+  CK(e);
+  return 0;
+}
+
+int xtg_forward_project(xtg_ctx *c, float *ax) {
+  if (!c) return XTG_E_ARG;
+  if (!c->d_ax && dalloc(c, &c->d_ax, c->ns)) return XTG_E_CUDA;
+  CK(launch_fp<0>(c, c->d_ax, nullptr));
+  if (ax) CK(cudaMemcpyAsync(ax, c->d_ax, c->ns * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int xtg_init_error_sino(xtg_ctx *c) {
+  if (!c) return XTG_E_ARG;
+  if (!c->have_sino) {
+    set_err("xtg_init_error_sino: no sinogram uploaded");
+    return XTG_E_STATE;
+  }
+  CK(launch_fp<1>(c, c->d_e, nullptr));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+static int finish_cost(xtg_ctx *c, double data_sum, double *cost, double *fwd, double *prior);
+
+int xtg_resync_fp64(xtg_ctx *c, double *cost, double *fwd, double *prior) {
+  if (!c) return XTG_E_ARG;
+  if (!c->have_sino) {
+    set_err("xtg_resync_fp64: no sinogram uploaded");
+    return XTG_E_STATE;
+  }
+  CK(cudaMemsetAsync(c->d_red, 0, NSLOT * 8, c->st));
+  CK(launch_fp<2>(c, c->d_e, c->d_red));
+  if (!cost && !fwd && !prior) {
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+  }
+  double h[NSLOT];
+  CK(cudaMemcpyAsync(h, c->d_red, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double s = 0;
+  for (int i = 0; i < NSLOT; i++) s += h[i];
+  return finish_cost(c, s, cost, fwd, prior);
+}
+
+static int finish_cost(xtg_ctx *c, double data_sum, double *cost, double *fwd, double *prior) {
+  CK(cudaMemsetAsync(c->d_red + NSLOT, 0, NSLOT * 8, c->st));
+  const unsigned grid = std::min<unsigned>(blocks_for(c->nvox, 256), (unsigned)c->sm_count * 8);
+  k_prior_cost64<<<grid, 256, 0, c->st>>>(c->G, c->d_x, c->d_red + NSLOT);
+  c->launches++;
+  CK(cudaGetLastError());
+  double h[NSLOT];
+  CK(cudaMemcpyAsync(h, c->d_red + NSLOT, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  float var = 0;
+  CK(cudaMemcpyAsync(&var, c->d_var, 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double pr = 0;
+  for (int i = 0; i < NSLOT; i++) pr += h[i];
+  const double f = data_sum / 2.0 + (double)c->g.N_p * c->g.N_r * c->g.N_t * log((double)var) / 2.0;
+  if (cost) *cost = f + pr;
+  if (fwd) *fwd = f;
+  if (prior) *prior = pr;
+  return 0;
+}
+
+int xtg_map_cost_fp64(xtg_ctx *c, double *cost, double *fwd, double *prior) {
+  if (!c) return XTG_E_ARG;
+  if (!c->have_sino) {
+    set_err("xtg_map_cost_fp64: no sinogram uploaded");
+    return XTG_E_STATE;
+  }
+  CK(cudaMemsetAsync(c->d_red, 0, NSLOT * 8, c->st));
+  CK(launch_fp<3>(c, nullptr, c->d_red));
+  double h[NSLOT];
+  CK(cudaMemcpyAsync(h, c->d_red, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double s = 0;
+  for (int i = 0; i < NSLOT; i++) s += h[i];
+  return finish_cost(c, s, cost, fwd, prior);
+}
+
+int xtg_map_cost_running(xtg_ctx *c, double *cost, double *fwd, double *prior) {
+  if (!c) return XTG_E_ARG;
+  CK(cudaMemsetAsync(c->d_red, 0, NSLOT * 8, c->st));
+  const unsigned grid = std::min<unsigned>(blocks_for(c->ns, 256), (unsigned)c->sm_count * 8);
+  k_running_cost64<<<grid, 256, 0, c->st>>>(c->ns, c->d_e, c->d_w, c->g.T, c->g.delta, c->d_red);
+  c->launches++;
+  CK(cudaGetLastError());
+  double h[NSLOT];
+  CK(cudaMemcpyAsync(h, c->d_red, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double s = 0;
+  for (int i = 0; i < NSLOT; i++) s += h[i];
+  return finish_cost(c, s, cost, fwd, prior);
+}
+
+int xtg_zinger_refresh(xtg_ctx *c, uint8_t *sel, int64_t *nsel) {
+  if (!c) return XTG_E_ARG;
+  unsigned char *ds = nullptr;
+  if (sel) CK(cudaMalloc(&ds, c->ns));
+  CK(cudaMemsetAsync(c->d_cnt + 3, 0, 8, c->st));
+  const unsigned grid = std::min<unsigned>(blocks_for(c->ns, 256), (unsigned)c->sm_count * 8);
+  k_zinger_refresh<<<grid, 256, 0, c->st>>>(c->ns, c->d_e, c->d_w, c->g.T, ds, c->d_cnt + 3);
+  c->launches++;
+  unsigned long long h = 0;
+  cudaMemcpyAsync(&h, c->d_cnt + 3, 8, cudaMemcpyDeviceToHost, c->st);
+  if (sel) cudaMemcpyAsync(sel, ds, c->ns, cudaMemcpyDeviceToHost, c->st);
+  cudaError_t e = cudaStreamSynchronize(c->st);
+  if (ds) cudaFree(ds);
+  CK(e);
+  if (nsel) *nsel = (int64_t)h;
+  return 0;
+}
+
+int xtg_update_offset(xtg_ctx *c) {
+  if (!c) return XTG_E_ARG;
+  CK(cudaMemsetAsync(c->d_red + 2 * NSLOT, 0, 2 * 8, c->st));
+  const unsigned grid = blocks_for(c->nrt, 128);
+  k_offset_numden<<<grid, 128, 0, c->st>>>(c->G, c->d_e, c->d_w, c->d_d, c->d_num, c->d_den, c->d_red + 2 * NSLOT);
+  k_offset_apply<<<grid, 128, 0, c->st>>>(c->G, c->d_e, c->d_d, c->d_num, c->d_den, c->d_red + 2 * NSLOT,
+                                          c->prm.EnforceZeroMeanOffset);
+  c->launches += 2;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int xtg_update_variance(xtg_ctx *c) {
+  if (!c) return XTG_E_ARG;
+  CK(cudaMemsetAsync(c->d_red + 3 * NSLOT, 0, NSLOT * 8, c->st));
+  const unsigned grid = std::min<unsigned>(blocks_for(c->ns, 256), (unsigned)c->sm_count * 8);
+  k_var_sum<<<grid, 256, 0, c->st>>>(c->ns, c->d_e, c->d_w, c->d_var, c->g.T, c->g.delta, c->d_red + 3 * NSLOT);
+  k_var_finish<<<1, 32, 0, c->st>>>(c->d_red + 3 * NSLOT, (double)c->ns, c->d_var);
+  k_scale_weights<<<grid, 256, 0, c->st>>>(c->ns, c->d_w, c->d_var);
+  c->launches += 3;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// ------------------------------------------------------------ ICD driver --
+static int ensure_a16(xtg_ctx *c) {
+  if (c->a16_ok) return 0;
+  c->a16_vmax = c->vmax;
+  const size_t nrec = (size_t)c->g.N_time * c->n_masked * c->a16_vmax;
+  if (!c->d_a16 && dalloc(c, &c->d_a16, nrec)) return XTG_E_CUDA;
+  if (!c->d_a16s && dalloc(c, &c->d_a16s, (size_t)c->g.N_time * c->n_masked)) return XTG_E_CUDA;
+  const long long warps = (long long)c->g.N_time * c->n_masked;
+  k_build_a16<<<(unsigned)((warps + 7) / 8), 256, 0, c->st>>>(c->G, c->d_hr, c->d_cos, c->d_sin, c->d_view_idx,
+                                                             c->d_view_start, c->d_view_num, c->n_masked, c->d_mcols,
+                                                             c->a16_vmax, c->d_a16, c->d_a16s);
+  c->launches++;
+  CK(cudaGetLastError());
+  c->a16_ok = 1;
+  return 0;
+}
+
+// one ICD launch over items[lo, lo+n) (or a device-counted list)
+static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, const int *n_dev, int use_perm,
+                       unsigned long long key, int whole_lines, int seq_override) {
+  const xt_geom &g = c->g;
+  if (c->a_mode == XTG_A_FP16) {
+    int rc = ensure_a16(c);
+    if (rc) return rc;
+  }
+  const int seq = (seq_override >= 0) ? seq_override : (c->order == XTG_ORDER_SEQUENTIAL);
+  // rows of one work item: a whole z-line, or one z-block (the last block is the longest)
+  const int zmax = whole_lines ? g.N_z : (g.N_z - (g.nzb - 1) * g.zstep);
+  const int rows = zmax * g.zovl;
+  bool v4 = (g.N_t % 4 == 0);
+  if (!whole_lines) v4 = v4 && ((g.zstep * g.zovl) % 4 == 0) && (rows % 4 == 0);
+  const int vec = v4 ? 4 : 1;
+  if ((rows + vec - 1) / vec > 32) {
+    set_err("ICD work item of %d detector rows exceeds the kernel's %d (N_z/nzb too large)", rows, 32 * vec);
+    return XTG_E_ARG;
+  }
+  const int span = (int)ceil(2.0 * g.delta_xy / g.delta_r) + 1;
+  const int as = span <= 4 ? 4 : 12;
+  if (span > 12) {
+    set_err("delta_xy too large for the ICD kernel (%d bins per view)", span);
+    return XTG_E_ARG;
+  }
+  const int amode = (c->a_mode == XTG_A_FP16) ? 1 : 0;
+  IcdArgs A;
+  memset(&A, 0, sizeof(A));
+  A.e = c->d_e; A.w = c->d_w; A.x = c->d_x; A.magmap = c->d_mag; A.hr = c->d_hr; A.cosv = c->d_cos;
+  A.sinv = c->d_sin; A.view_idx = c->d_view_idx; A.view_start = c->d_view_start; A.view_num = c->d_view_num;
+  A.items = items; A.n_items_dev = n_dev; A.n_items = n; A.item_lo = lo; A.counter = c->d_counter;
+  A.use_perm = use_perm; A.perm_key = key; A.a16 = c->d_a16; A.a16_scale = c->d_a16s; A.col_rank = c->d_rank;
+  A.a16_vmax = c->a16_vmax; A.n_masked = c->n_masked; A.iter = iter;
+  A.T2 = g.T * g.T; A.Tdelta = g.T * g.delta; A.st_absx = c->d_absx; A.st_cnt = c->d_cnt; A.err = c->d_err;
+  int grid;
+  if (seq) {
+    grid = 1;
+  } else {
+    const int occ = icd_occupancy(vec, amode, 0, as, c->vmax, zmax, g.zovl);
+    grid = c->sm_count * occ;
+    if (c->max_columns > 0) grid = std::min(grid, c->max_columns);
+    if (!n_dev) grid = std::min(grid, std::max(n, 1));
+  }
+  CK(cudaMemsetAsync(c->d_counter, 0, 4, c->st));
+  CK(launch_icd(c->G, A, vec, amode, seq, as, c->vmax, zmax, grid, c->st));
+  c->launches++;
+  return 0;
+}
+
+static void magsum_launch(xtg_ctx *c) {
+  const size_t n = (size_t)c->g.N_time * c->g.nzb * c->n_masked;
+  const unsigned grid = std::min<unsigned>(blocks_for(n, 256), (unsigned)c->sm_count * 4);
+  k_magsum<<<std::max(grid, 1u), 256, 0, c->st>>>(c->G, c->n_masked, c->d_mcols, c->d_mag, c->d_red + 4 * NSLOT);
+  c->launches++;
+}
+
+// NHICD selection on the device: filter, per-(frame, block) order statistic,
+// compaction into the two half-pass lists.
+static int nhicd_select_device(xtg_ctx *c) {
+  const xt_geom &g = c->g;
+  const int nseg = g.N_time * g.nzb;
+  const int nsel = c->n_masked / XT_NHICD_CHUNKS;
+  std::vector<int> kth(nseg, (int)c->nxy - nsel);
+  CK(cudaMemcpyAsync(c->d_kth, kth.data(), nseg * 4, cudaMemcpyHostToDevice, c->st));
+  const unsigned grid = std::min<unsigned>(blocks_for(c->nmag, 256), (unsigned)c->sm_count * 8);
+  k_vsc_filter<<<grid, 256, 0, c->st>>>(nseg, g.N_y, g.N_x, c->d_mag, c->d_filt);
+  k_radix_select<<<nseg, 1024, 0, c->st>>>(c->d_filt, (int)c->nxy, c->d_kth, c->d_thr);
+  CK(cudaMemsetAsync(c->d_nhcnt, 0, 8, c->st));
+  const int cap0 = (int)(c->nh_cap / 2), cap1 = (int)(c->nh_cap - c->nh_cap / 2);
+  k_nhicd_compact<<<grid, 256, 0, c->st>>>(g.N_time, g.nzb, g.N_y, g.N_x, c->d_filt, c->d_thr, c->d_nh,
+                                           c->d_nh + cap0, c->d_nhcnt, cap0, cap1);
+  k_clamp_count<<<1, 32, 0, c->st>>>(c->d_nhcnt, cap0, cap1);
+  c->launches += 4;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int read_stats(xtg_ctx *c, xtg_stats *st, double *absx_out) {
+  double ab[NSLOT];
+  unsigned long long cnt[3];
+  CK(cudaMemcpyAsync(ab, c->d_absx, sizeof(ab), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(cnt, c->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double s = 0;
+  for (int i = 0; i < NSLOT; i++) s += ab[i];
+  if (absx_out) *absx_out = s;
+  if (st) {
+    st->voxel_updates += (int64_t)cnt[0];
+    st->zero_skipped += (int64_t)cnt[1];
+    st->columns += (int64_t)cnt[2];
+  }
+  return 0;
+}
+
+static int reset_stats(xtg_ctx *c) {
+  CK(cudaMemsetAsync(c->d_absx, 0, NSLOT * 8, c->st));
+  CK(cudaMemsetAsync(c->d_cnt, 0, 3 * 8, c->st));
+  return 0;
+}
+
+// Reference-order random lists (randomly_select_x_y, XT_ICD_update.c:599-631)
+// drawn with the reference generator, for the sequential parity mode.
+static void host_random_lists(xtg_ctx *c, std::vector<int> &usn, std::vector<int> &xs, std::vector<int> &ys) {
+  const xt_geom &g = c->g;
+  const int nxy = (int)c->nxy;
+  usn.assign((size_t)g.N_time * g.nzb, 0);
+  xs.assign((size_t)g.N_time * g.nzb * nxy, 0);
+  ys.assign((size_t)g.N_time * g.nzb * nxy, 0);
+  std::vector<int> counter(nxy);
+  for (int i = 0; i < g.N_time; i++)
+    for (int b = 0; b < g.nzb; b++) {
+      int size = nxy;
+      int &u = usn[(size_t)i * g.nzb + b];
+      for (int q = 0; q < nxy; q++) counter[q] = q;
+      for (int jj = 0; jj < nxy; jj++) {
+        int index = (int)floor(rng_next(c) * size);
+        index = (index == size) ? size - 1 : index;
+        const int col = counter[index] % g.N_x, row = counter[index] / g.N_x;
+        if (c->col_rank[(size_t)row * g.N_x + col] >= 0) {
+          xs[((size_t)i * g.nzb + b) * nxy + u] = col;
+          ys[((size_t)i * g.nzb + b) * nxy + u] = row;
+          u++;
+        }
+        counter[index] = counter[size - 1];
+        size--;
+      }
+    }
+}
+
+// RandomizedSelect with the reference generator (XT_NHICD.c:63-126), used in
+// the sequential mode so later iterations draw the reference's numbers.
+static float host_randomized_select(xtg_ctx *c, float *A, unsigned p, unsigned r, unsigned i) {
+  for (;;) {
+    if (p == r) return A[p];
+    unsigned rnum = (unsigned)floor(rng_next(c) * (r - p + 1));
+    rnum = (rnum == r - p + 1) ? r - p : rnum;
+    const unsigned j = p + rnum;
+    std::swap(A[r], A[j]);
+    const float x = A[r];
+    unsigned ii = p - 1;
+    for (unsigned jj = p; jj < r; jj++)
+      if (A[jj] <= x) {
+        ii++;
+        std::swap(A[ii], A[jj]);
+      }
+    std::swap(A[ii + 1], A[r]);
+    const unsigned q = ii + 1, k = q - p + 1;
+    if (i == k) return A[q];
+    if (i < k)
+      r = q - 1;
+    else {
+      p = q + 1;
+      i -= k;
+    }
+  }
+}
+
+static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
+  const xt_geom &g = c->g;
+  const int n = g.N_time * c->n_masked;
+  const unsigned long long key = c->seed * 0x9E3779B97F4A7C15ULL + (unsigned long long)iter * 0xD1B54A32D192ED03ULL;
+  k_build_items<<<blocks_for(n, 256), 256, 0, c->st>>>(n, c->n_masked, g.N_x, c->d_mcols, key, c->d_items);
+  c->launches++;
+  CK(cudaGetLastError());
+  const int K = XT_NHICD_CHUNKS, chunk = n / K;
+  const int cap0 = (int)(c->nh_cap / 2);
+  float kms_total = 0.f;
+  long long items_total = 0;
+  double vox_mag = 0;
+  for (int j = 0; j < K; j++) {
+    const int lo = j * chunk, hi = (j == K - 1) ? n : (j + 1) * chunk;
+    if (j == K - 1) {  // the reference's vox_mag covers the last chunk only (XT_ICD_update.c:798)
+      double tmp;
+      int rc = read_stats(c, st, &tmp);
+      if (rc) return rc;
+      rc = reset_stats(c);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(c->ek0, c->st));
+    int rc = run_columns(c, iter, c->d_items, lo, hi - lo, nullptr, 0, 0, 1, -1);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ek1, c->st));
+    if (j == K - 1) {
+      rc = read_stats(c, st, &vox_mag);
+      if (rc) return rc;
+      rc = reset_stats(c);
+      if (rc) return rc;
+    }
+    CK(cudaEventSynchronize(c->ek1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ek0, c->ek1));
+    kms_total += ms;
+    items_total += hi - lo;
+    if (c->prm.updateProjOffset > 1) {
+      rc = xtg_update_offset(c);
+      if (rc) return rc;
+    }
+    rc = nhicd_select_device(c);
+    if (rc) return rc;
+    if (iter > 1 && !c->prm.no_NHICD) {
+      for (int h = 0; h < 2; h++) {
+        CK(cudaEventRecord(c->ek0, c->st));
+        rc = run_columns(c, iter, c->d_nh, h ? cap0 : 0, 0, c->d_nhcnt + h, 1, key + 17 * (j * 2 + h + 1), 0, -1);
+        if (rc) return rc;
+        CK(cudaEventRecord(c->ek1, c->st));
+        CK(cudaEventSynchronize(c->ek1));
+        float ms2 = 0;
+        CK(cudaEventElapsedTime(&ms2, c->ek0, c->ek1));
+        kms_total += ms2;
+        if (c->prm.updateProjOffset > 1) {
+          rc = xtg_update_offset(c);
+          if (rc) return rc;
+        }
+      }
+    }
+  }
+  int hc[2];
+  CK(cudaMemcpyAsync(hc, c->d_nhcnt, 8, cudaMemcpyDeviceToHost, c->st));
+  double tmp;
+  int rc = read_stats(c, st, &tmp);
+  if (rc) return rc;
+  c->last_kms = kms_total;
+  c->last_items = items_total;
+  st->vox_mag = vox_mag;
+  return 0;
+}
+
+static int icd_iteration_sequential(xtg_ctx *c, int iter, xtg_stats *st) {
+  const xt_geom &g = c->g;
+  const int nxy = (int)c->nxy, K = XT_NHICD_CHUNKS;
+  std::vector<int> usn, xs, ys;
+  host_random_lists(c, usn, xs, ys);
+  std::vector<int4> items;
+  double vox_mag = 0;
+  float kms_total = 0;
+  long long items_total = 0;
+  auto run_list = [&](std::vector<int4> &L) -> int {
+    if (L.empty()) return 0;
+    if (L.size() > c->items_cap) {
+      set_err("work list too long");
+      return XTG_E_ARG;
+    }
+    CK(cudaMemcpyAsync(c->d_items, L.data(), L.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
+    CK(cudaEventRecord(c->ek0, c->st));
+    int rc = run_columns(c, iter, c->d_items, 0, (int)L.size(), nullptr, 0, 0, 0, 1);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ek1, c->st));
+    CK(cudaEventSynchronize(c->ek1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ek0, c->ek1));
+    kms_total += ms;
+    items_total += (long long)L.size();
+    return 0;
+  };
+  std::vector<float> filt((size_t)nxy), filtc((size_t)nxy);
+  std::vector<int> nsn((size_t)g.N_time * g.nzb);
+  std::vector<int> xn((size_t)g.N_time * g.nzb * nxy), yn((size_t)g.N_time * g.nzb * nxy);
+  for (int j = 0; j < K; j++) {
+    if (j == K - 1) {
+      double tmp;
+      int rc = read_stats(c, st, &tmp);
+      if (rc) return rc;
+      rc = reset_stats(c);
+      if (rc) return rc;
+    }
+    for (int half = 0; half < 2; half++) {
+      items.clear();
+      for (int i = 0; i < g.N_time; i++)
+        for (int b = 0; b < g.nzb; b += 2) {
+          const int idx = (((i % 2) == 0) ^ half) ? b : b + 1;
+          const int u = usn[(size_t)i * g.nzb + idx];
+          const int xb = j * (int)floor(u / K);
+          const int xe = (j == K - 1) ? u - 1 : (j + 1) * (int)floor(u / K) - 1;
+          for (int q = xb; q <= xe; q++)
+            items.push_back(make_int4(i, ys[((size_t)i * g.nzb + idx) * nxy + q], xs[((size_t)i * g.nzb + idx) * nxy + q], idx));
+        }
+      int rc = run_list(items);
+      if (rc) return rc;
+      if (c->prm.updateProjOffset > 1) {
+        rc = xtg_update_offset(c);
+        if (rc) return rc;
+      }
+    }
+    if (j == K - 1) {
+      int rc = read_stats(c, st, &vox_mag);
+      if (rc) return rc;
+      rc = reset_stats(c);
+      if (rc) return rc;
+    }
+    // NHICD selection with the reference's RandomizedSelect on the device-filtered map
+    const int nseg = g.N_time * g.nzb;
+    const unsigned grid = std::min<unsigned>(blocks_for(c->nmag, 256), (unsigned)c->sm_count * 8);
+    k_vsc_filter<<<grid, 256, 0, c->st>>>(nseg, g.N_y, g.N_x, c->d_mag, c->d_filt);
+    c->launches++;
+    std::vector<float> allf(c->nmag);
+    CK(cudaMemcpyAsync(allf.data(), c->d_filt, c->nmag * 4, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int s = 0; s < nseg; s++) {
+      const int n = (int)floor(usn[s] / XT_NHICD_CHUNKS);
+      memcpy(filt.data(), &allf[(size_t)s * nxy], (size_t)nxy * 4);
+      memcpy(filtc.data(), filt.data(), (size_t)nxy * 4);
+      const float th = host_randomized_select(c, filt.data(), 0, (unsigned)(nxy - 1), (unsigned)(nxy - n));
+      int idx = 0;
+      for (int r = 0; r < g.N_y; r++)
+        for (int k = 0; k < g.N_x; k++)
+          if (filtc[(size_t)r * g.N_x + k] > th) {
+            xn[(size_t)s * nxy + idx] = k;
+            yn[(size_t)s * nxy + idx] = r;
+            idx++;
+          }
+      nsn[s] = idx;
+    }
+    if (iter > 1 && !c->prm.no_NHICD) {
+      for (int half = 0; half < 2; half++) {
+        items.clear();
+        for (int i = 0; i < g.N_time; i++)
+          for (int b = 0; b < g.nzb; b += 2) {
+            const int idx = (((i % 2) == 0) ^ half) ? b : b + 1;
+            const int s = i * g.nzb + idx;
+            for (int q = 0; q < nsn[s]; q++) items.push_back(make_int4(i, yn[(size_t)s * nxy + q], xn[(size_t)s * nxy + q], idx));
+          }
+        int rc = run_list(items);
+        if (rc) return rc;
+        if (c->prm.updateProjOffset > 1) {
+          rc = xtg_update_offset(c);
+          if (rc) return rc;
+        }
+      }
+    }
+  }
+  double tmp;
+  int rc = read_stats(c, st, &tmp);
+  if (rc) return rc;
+  c->last_kms = kms_total;
+  c->last_items = items_total;
+  st->vox_mag = vox_mag;
+  return 0;
+}
+
+int xtg_icd_iteration(xtg_ctx *c, int32_t iter, xtg_stats *st_out) {
+  if (!c) return XTG_E_ARG;
+  if (!c->have_sino) {
+    set_err("xtg_icd_iteration: no sinogram uploaded");
+    return XTG_E_STATE;
+  }
+  xtg_stats st;
+  memset(&st, 0, sizeof(st));
+  int rc = reset_stats(c);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev0, c->st));
+  rc = (c->order == XTG_ORDER_SEQUENTIAL) ? icd_iteration_sequential(c, iter, &st) : icd_iteration_parallel(c, iter, &st);
+  if (rc) return rc;
+  if (c->prm.do_VarEst) {
+    rc = xtg_update_variance(c);
+    if (rc) return rc;
+  }
+  // stop statistic (XT_ICD_update.c:884-925)
+  CK(cudaMemsetAsync(c->d_red + 4 * NSLOT, 0, NSLOT * 8, c->st));
+  magsum_launch(c);
+  CK(cudaGetLastError());
+  double h[NSLOT];
+  CK(cudaMemcpyAsync(h, c->d_red + 4 * NSLOT, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaEventRecord(c->ev1, c->st));
+  CK(cudaEventSynchronize(c->ev1));
+  CK(cudaEventElapsedTime(&st.ms, c->ev0, c->ev1));
+  double ms = 0;
+  for (int i = 0; i < NSLOT; i++) ms += h[i];
+  st.mag_sum = ms;
+  st.total_pix = (double)c->n_masked * c->g.N_time * c->g.nzb * (double)(c->g.N_z / c->g.nzb);
+  st.avg_update_pct = (st.vox_mag > 0) ? 100.0 * ms / st.vox_mag : INFINITY;
+  st.converged = st.avg_update_pct < (double)c->g.StopThreshold;
+  rc = check_err_flag(c);
+  if (rc) return rc;
+  if (st_out) *st_out = st;
+  return 0;
+}
+
+int xtg_update_columns(xtg_ctx *c, int32_t iter, int32_t n, const int32_t *items, xtg_stats *st_out) {
+  if (!c || n < 0 || (n && !items)) return XTG_E_ARG;
+  if (!c->have_sino) {
+    set_err("xtg_update_columns: no sinogram uploaded");
+    return XTG_E_STATE;
+  }
+  if ((size_t)n > c->items_cap) {
+    set_err("xtg_update_columns: %d items exceed the list capacity %zu", n, c->items_cap);
+    return XTG_E_ARG;
+  }
+  const xt_geom &g = c->g;
+  int whole = 1;
+  for (int q = 0; q < n; q++) {
+    const int f = items[4 * q], r = items[4 * q + 1], k = items[4 * q + 2], b = items[4 * q + 3];
+    if (f < 0 || f >= g.N_time || r < 0 || r >= g.N_y || k < 0 || k >= g.N_x || b < -1 || b >= g.nzb) {
+      set_err("xtg_update_columns: item %d out of range", q);
+      return XTG_E_ARG;
+    }
+    if (c->a_mode == XTG_A_FP16 && c->col_rank[(size_t)r * g.N_x + k] < 0) {
+      set_err("xtg_update_columns: FP16 A covers masked columns only (item %d)", q);
+      return XTG_E_ARG;
+    }
+    if (b >= 0) whole = 0;
+  }
+  xtg_stats st;
+  memset(&st, 0, sizeof(st));
+  int rc = reset_stats(c);
+  if (rc) return rc;
+  if (n) CK(cudaMemcpyAsync(c->d_items, items, (size_t)n * sizeof(int4), cudaMemcpyHostToDevice, c->st));
+  CK(cudaEventRecord(c->ek0, c->st));
+  rc = run_columns(c, iter, c->d_items, 0, n, nullptr, 0, 0, whole, -1);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ek1, c->st));
+  double ab = 0;
+  rc = read_stats(c, &st, &ab);
+  if (rc) return rc;
+  CK(cudaEventElapsedTime(&st.ms, c->ek0, c->ek1));
+  st.vox_mag = ab;
+  c->last_kms = st.ms;
+  c->last_items = n;
+  rc = check_err_flag(c);
+  if (rc) return rc;
+  if (st_out) *st_out = st;
+  return 0;
+}
+
+int xtg_nhicd_select(xtg_ctx *c, const int32_t *usn, int32_t *nnum, int32_t *xsel, int32_t *ysel, float *thr) {
+  if (!c || !usn || !nnum) return XTG_E_ARG;
+  const xt_geom &g = c->g;
+  const int nseg = g.N_time * g.nzb;
+  std::vector<int> kth(nseg);
+  for (int s = 0; s < nseg; s++) kth[s] = (int)c->nxy - (int)floor(usn[s] / XT_NHICD_CHUNKS);
+  for (int s = 0; s < nseg; s++)
+    if (kth[s] < 1 || kth[s] > (int)c->nxy) {
+      set_err("xtg_nhicd_select: update_select_num out of range");
+      return XTG_E_ARG;
+    }
+  CK(cudaMemcpyAsync(c->d_kth, kth.data(), nseg * 4, cudaMemcpyHostToDevice, c->st));
+  const unsigned grid = std::min<unsigned>(blocks_for(c->nmag, 256), (unsigned)c->sm_count * 8);
+  k_vsc_filter<<<grid, 256, 0, c->st>>>(nseg, g.N_y, g.N_x, c->d_mag, c->d_filt);
+  k_radix_select<<<nseg, 1024, 0, c->st>>>(c->d_filt, (int)c->nxy, c->d_kth, c->d_thr);
+  c->launches += 2;
+  CK(cudaGetLastError());
+  std::vector<float> th(nseg), f(c->nmag);
+  CK(cudaMemcpyAsync(th.data(), c->d_thr, nseg * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(f.data(), c->d_filt, c->nmag * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  // lists in the reference's raster order
+  for (int s = 0; s < nseg; s++) {
+    int idx = 0;
+    for (int r = 0; r < g.N_y; r++)
+      for (int k = 0; k < g.N_x; k++)
+        if (f[(size_t)s * c->nxy + (size_t)r * g.N_x + k] > th[s]) {
+          if (xsel) xsel[(size_t)s * c->nxy + idx] = k;
+          if (ysel) ysel[(size_t)s * c->nxy + idx] = r;
+          idx++;
+        }
+    nnum[s] = idx;
+    if (thr) thr[s] = th[s];
+  }
+  return 0;
+}
+
+int64_t xtg_device_bytes(const xtg_ctx *c) { return c ? (int64_t)c->dev_bytes : 0; }
+int64_t xtg_launch_count(const xtg_ctx *c) { return c ? (int64_t)c->launches : 0; }
+
+int xtg_last_kernel_time(const xtg_ctx *c, float *ms, int64_t *items, int64_t *rows) {
+  if (!c) return XTG_E_ARG;
+  if (ms) *ms = c->last_kms;
+  if (items) *items = c->last_items;
+  if (rows) *rows = c->last_rows;
+  return 0;
+}
+
+}  // extern "C"

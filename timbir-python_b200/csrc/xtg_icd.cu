@@ -1,0 +1,360 @@
+// xtg_icd.cu -- the ICD column kernel: one CTA updates one x-y column's
+// z-line (or one z-block of it) of one time frame.
+//
+// Parallel-beam A is z-invariant: every slice of a column sees the same
+// (view, bin) entries, and the rows of slice z are t = z*zovl .. z*zovl+zovl-1.
+// So the CTA computes the column's A once into shared memory, then streams
+// the column's footprint e[p][bin][t0..t0+T) and w[...] (contiguous in t) with
+// vector loads, thread (view-group, t-lane) accumulating theta1/theta2 for its
+// rows; shuffles and a shared-memory pass reduce them over view groups.  The
+// slices' qGGMRF surrogate steps run in red/black z order (or strictly in
+// increasing z, the reference's order, in sequential mode), and the e update
+// goes back with vector red.global.add, so columns in flight that share
+// sinogram entries never lose an update.
+//
+// Reference: updateVoxels_Aditya + compute_voxel_update_Aditya
+// (Source_Code_4D_Fast/XT_VoxUpdate.c:11-254), CE_FunctionalSubstitution
+// (XT_ICD_update.c:130-179); the z-line batching follows updateVoxels_AttTomo
+// (XT_VoxUpdate.c:266-586).
+#include "xtg_internal.h"
+
+namespace xtg {
+
+
+template <int VEC, int AMODE, int SEQ, int AS>
+__global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArgs A, int vmax, int zmax) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int *sPack = reinterpret_cast<int *>(smem_raw);               // [vmax] first | cnt << 24
+  int *sView = sPack + vmax;                                     // [vmax] view index p
+  float *sVal = reinterpret_cast<float *>(sView + vmax);         // [vmax * AS] A * delta_t
+  float *sRed = sVal + (size_t)vmax * AS;                    // [2][8][128] warp partials
+  float *sTh = sRed + 2 * 8 * 128;                               // [2][zmax*zovl]
+  const int rowsmax = zmax * G.zovl;
+  float *sNb = sTh + 2 * rowsmax;                                // [9][zmax+2]
+  float *sTn = sNb + 9 * (zmax + 2);                             // [2][zmax]
+  float *sDelta = sTn + 2 * zmax;                                // [zmax]
+  __shared__ int sItem;
+  __shared__ double sAbs[XTG_THREADS / 32];
+  __shared__ unsigned sUpd, sZero;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nitems = A.n_items_dev ? *A.n_items_dev : A.n_items;
+
+  for (;;) {
+    if (tid == 0) {
+      sItem = atomicAdd(A.counter, 1);
+      sUpd = 0;
+      sZero = 0;
+    }
+    __syncthreads();
+    const int it = sItem;
+    if (it >= nitems) break;
+    const int q = A.use_perm ? (int)xt_perm((uint32_t)it, (uint32_t)nitems, A.perm_key) : it;
+    const int4 item = A.items[A.item_lo + q];
+    const int fr = item.x, row = item.y, col = item.z, blk = item.w;
+    int zb = 0, ze = G.N_z - 1;
+    if (blk >= 0) {
+      zb = blk * G.zstep;
+      ze = (blk >= G.nzb - 1) ? G.N_z - 1 : (blk + 1) * G.zstep - 1;
+    }
+    const int Z = ze - zb + 1, T = Z * G.zovl, t0 = zb * G.zovl;
+    const int V = A.view_num[fr], vs = A.view_start[fr];
+
+    // 1. the column's A entries (times delta_t, XT_VoxUpdate.c:27) -> smem
+    if (AMODE == 0) {
+      for (int v = tid; v < V; v += XTG_THREADS) {
+        const int p = A.view_idx[vs + v];
+        float vals[XT_AMAX];
+        int first;
+        const int n = xt_amatrix_view(G, A.hr + (size_t)p * XT_HR_STRIDE, A.cosv[p], A.sinv[p], row, col, vals, &first);
+        sPack[v] = first | (min(n, AS) << 24);
+        sView[v] = p;
+#pragma unroll
+        for (int s = 0; s < AS; s++) sVal[v * AS + s] = (s < n) ? __fmul_rn(vals[s], G.delta_t) : 0.f;
+      }
+    } else {
+      const int rk = A.col_rank[row * G.N_x + col];
+      const size_t rec = ((size_t)fr * A.n_masked + rk) * A.a16_vmax;
+      const float sc = A.a16_scale[(size_t)fr * A.n_masked + rk];
+      for (int v = tid; v < V; v += XTG_THREADS) {
+        const uint4 r4 = A.a16[rec + v];
+        const int first = (int)(r4.x & 0xffffu), n = (int)((r4.x >> 16) & 0xffu);
+        sPack[v] = first | (n << 24);
+        sView[v] = A.view_idx[vs + v];
+        const __half2 h01 = *reinterpret_cast<const __half2 *>(&r4.y);
+        const __half2 h23 = *reinterpret_cast<const __half2 *>(&r4.z);
+        sVal[v * AS + 0] = __low2float(h01) * sc;
+        sVal[v * AS + 1] = __high2float(h01) * sc;
+        sVal[v * AS + 2] = __low2float(h23) * sc;
+        sVal[v * AS + 3] = __high2float(h23) * sc;
+      }
+    }
+    // 2. neighbourhood: the 3x3 columns' z-lines over [zb-1, ze+1], and the
+    //    same column in frames fr-1 and fr+1 (0 outside the volume)
+    const size_t plane = (size_t)G.N_y * G.N_x;
+    for (int k = tid; k < 9 * (Z + 2); k += XTG_THREADS) {
+      const int c = k / (Z + 2), zz = k - c * (Z + 2);
+      const int jj = row + c / 3 - 1, kk = col + c % 3 - 1, za = zb - 1 + zz;
+      float v = 0.f;
+      if (jj >= 0 && jj < G.N_y && kk >= 0 && kk < G.N_x && za >= 0 && za < G.N_z)
+        v = A.x[(((size_t)fr * plane) + (size_t)jj * G.N_x + kk) * G.N_z + za];
+      sNb[c * (zmax + 2) + zz] = v;
+    }
+    for (int k = tid; k < 2 * Z; k += XTG_THREADS) {
+      const int s = k / Z, z = k - s * Z, f2 = fr + (s ? 1 : -1);
+      float v = 0.f;
+      if (f2 >= 0 && f2 < G.N_time) v = A.x[(((size_t)f2 * plane) + (size_t)row * G.N_x + col) * G.N_z + zb + z];
+      sTn[s * zmax + z] = v;
+    }
+    __syncthreads();
+
+    // 3. theta1 / theta2 over the column's footprint (XT_VoxUpdate.c:20-51)
+    const int tln = (T + VEC - 1) / VEC;
+    int tlp = 1;
+    while (tlp < tln) tlp <<= 1;
+    const int vgs = XTG_THREADS / tlp, tl = tid & (tlp - 1), vg = tid / tlp;
+    float th1[VEC], th2[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; c++) th1[c] = th2[c] = 0.f;
+    if (tl < tln) {
+      const int trow = t0 + tl * VEC;
+      for (int v = vg; v < V; v += vgs) {
+        const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
+        const size_t base = ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
+#pragma unroll
+        for (int s = 0; s < AS; s++) {
+          if (s < n) {
+            const float a = sVal[v * AS + s];
+            float ev[VEC], wv[VEC];
+            if (VEC == 4) {
+              const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(A.e + base + (size_t)s * G.N_t));
+              const float4 w4 = __ldg(reinterpret_cast<const float4 *>(A.w + base + (size_t)s * G.N_t));
+              ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
+              wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
+            } else {
+#pragma unroll
+              for (int c = 0; c < VEC; c++) {
+                ev[c] = __ldcg(A.e + base + (size_t)s * G.N_t + c);
+                wv[c] = __ldg(A.w + base + (size_t)s * G.N_t + c);
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < VEC; c++) {
+              // generalized-Huber (zinger) weight: w where |e sqrt(w)| < T,
+              // else T delta sqrt(w)/|e| (XT_VoxUpdate.c:34-48)
+              float we = wv[c];
+              if (ev[c] * ev[c] * wv[c] >= A.T2) we = A.Tdelta * sqrtf(wv[c]) / fabsf(ev[c]);
+              th2[c] += a * a * we;
+              th1[c] -= ev[c] * a * we;
+            }
+          }
+        }
+      }
+    }
+    // reduce over view groups: lanes with equal tl inside a warp, then warps
+#pragma unroll
+    for (int c = 0; c < VEC; c++) {
+      for (int off = tlp; off < 32; off <<= 1) {
+        th1[c] += __shfl_xor_sync(0xffffffffu, th1[c], off);
+        th2[c] += __shfl_xor_sync(0xffffffffu, th2[c], off);
+      }
+    }
+    if (lane < tlp && tl < tln) {
+#pragma unroll
+      for (int c = 0; c < VEC; c++) {
+        sRed[warp * 128 + tl * VEC + c] = th1[c];
+        sRed[8 * 128 + warp * 128 + tl * VEC + c] = th2[c];
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < T; t += XTG_THREADS) {
+      float s1 = 0.f, s2 = 0.f;
+      for (int wq = 0; wq < XTG_THREADS / 32; wq++) {  // every warp wrote its partial (zeros if idle)
+        s1 += sRed[wq * 128 + t];
+        s2 += sRed[8 * 128 + wq * 128 + t];
+      }
+      sTh[t] = s1;
+      sTh[rowsmax + t] = s2;
+    }
+    __syncthreads();
+
+    // 4. qGGMRF surrogate step per slice (CE_FunctionalSubstitution,
+    //    XT_ICD_update.c:130-179) with zero skipping (XT_VoxUpdate.c:208-232)
+    double absx = 0.0;
+    auto update = [&](int z) {
+      const int zz = z + 1;
+      const float Vv = sNb[4 * (zmax + 2) + zz];
+      float t1 = 0.f, t2 = 0.f;
+      for (int r = 0; r < G.zovl; r++) {
+        t1 += sTh[z * G.zovl + r];
+        t2 += sTh[rowsmax + z * G.zovl + r];
+      }
+      const int za = zb + z;
+      const bool zdn = za - 1 >= 0, zup = za + 1 < G.N_z;
+      const bool tdn = fr - 1 >= 0, tup = fr + 1 < G.N_time;
+      if (Vv == 0.f && A.iter > 1) {
+        bool skip = !(sTn[z] > 0.f || sTn[zmax + z] > 0.f);
+        for (int c = 0; c < 9 && skip; c++)
+          for (int dz = 0; dz < 3; dz++)
+            if (sNb[c * (zmax + 2) + zz - 1 + dz] > 0.f) skip = false;
+        if (skip) {
+          sDelta[z] = 0.f;
+          atomicAdd(&sZero, 1u);
+          return;
+        }
+      }
+      float num = 0.f, den = 0.f;
+#pragma unroll
+      for (int dz = 0; dz < 3; dz++) {
+        if ((dz == 0 && !zdn) || (dz == 2 && !zup)) continue;
+#pragma unroll
+        for (int c = 0; c < 9; c++) {
+          if (dz == 1 && c == 4) continue;
+          const int jj = row + c / 3 - 1, kk = col + c % 3 - 1;
+          if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x) continue;
+          const float nv = sNb[c * (zmax + 2) + zz - 1 + dz];
+          const float b = G.SF[dz * 9 + c] * xt_qggmrf_coef(Vv - nv, G.Sigma_S_Q, G.Sigma_S_Q_P, G.C_S, G.MRF_P);
+          num += b * nv;
+          den += b;
+        }
+      }
+      if (tdn) {
+        const float nv = sTn[z];
+        const float b = G.TF * xt_qggmrf_coef(Vv - nv, G.Sigma_T_Q, G.Sigma_T_Q_P, G.C_T, G.MRF_P);
+        num += b * nv;
+        den += b;
+      }
+      if (tup) {
+        const float nv = sTn[zmax + z];
+        const float b = G.TF * xt_qggmrf_coef(Vv - nv, G.Sigma_T_Q, G.Sigma_T_Q_P, G.C_T, G.MRF_P);
+        num += b * nv;
+        den += b;
+      }
+      const float u = (num + t2 * Vv - t1) / (den + t2);
+      float nvx = Vv + G.alpha * (u - Vv);
+      if (G.positivity && nvx <= 0.f) nvx = 0.f;
+      if (!isfinite(nvx)) {
+        atomicExch(A.err, 1);
+        nvx = Vv;
+      }
+      sNb[4 * (zmax + 2) + zz] = nvx;
+      A.x[(((size_t)fr * plane) + (size_t)row * G.N_x + col) * G.N_z + za] = nvx;
+      sDelta[z] = nvx - Vv;
+      absx += (double)fabsf(nvx);
+      atomicAdd(&sUpd, 1u);
+    };
+    if (SEQ) {
+      if (tid == 0)
+        for (int z = 0; z < Z; z++) update(z);
+    } else {
+      for (int par = 0; par < 2; par++) {
+        for (int z = tid; z < Z; z += XTG_THREADS)
+          if (((zb + z) & 1) == par) update(z);
+        __syncthreads();
+      }
+    }
+    __syncthreads();
+
+    // 5. MagUpdateMap[frame][block][row][col] = sum |delta| over the block's
+    //    slices of this visit (XT_VoxUpdate.c:128, 236); sum |x| and counters
+    for (int b = tid; b < G.nzb; b += XTG_THREADS) {
+      const int bz0 = b * G.zstep, bz1 = (b >= G.nzb - 1) ? G.N_z - 1 : (b + 1) * G.zstep - 1;
+      if (bz0 >= zb && bz1 <= ze) {
+        float m = 0.f;
+        for (int z = bz0; z <= bz1; z++) m += fabsf(sDelta[z - zb]);
+        A.magmap[(((size_t)fr * G.nzb + b) * G.N_y + row) * G.N_x + col] = m;
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) absx += __shfl_xor_sync(0xffffffffu, absx, off);
+    if (lane == 0) sAbs[warp] = absx;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int wq = 0; wq < XTG_THREADS / 32; wq++) s += sAbs[wq];
+      atomicAdd(&A.st_absx[blockIdx.x & 63], s);
+      atomicAdd(&A.st_cnt[0], (unsigned long long)sUpd);
+      atomicAdd(&A.st_cnt[1], (unsigned long long)sZero);
+      atomicAdd(&A.st_cnt[2], 1ull);
+    }
+
+    // 6. e -= (A delta_t) * delta_x on the footprint (XT_VoxUpdate.c:62-82)
+    if (tl < tln) {
+      float dv[VEC];
+      bool any = false;
+#pragma unroll
+      for (int c = 0; c < VEC; c++) {
+        const int rr = tl * VEC + c;
+        dv[c] = (rr < T) ? sDelta[rr / G.zovl] : 0.f;
+        any |= (dv[c] != 0.f);
+      }
+      if (any) {
+        const int trow = t0 + tl * VEC;
+        for (int v = vg; v < V; v += vgs) {
+          const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
+          float *ep = A.e + ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
+#pragma unroll
+          for (int s = 0; s < AS; s++) {
+            if (s < n) {
+              const float a = sVal[v * AS + s];
+              if (VEC == 4) {
+                xt_red_add4(ep + (size_t)s * G.N_t, -(a * dv[0]), -(a * dv[1]), -(a * dv[2]), -(a * dv[3]));
+              } else {
+#pragma unroll
+                for (int c = 0; c < VEC; c++)
+                  if (dv[c] != 0.f) atomicAdd(ep + (size_t)s * G.N_t + c, -(a * dv[c]));
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as) {
+  size_t b = 0;
+  b += (size_t)vmax * 4 * 2;         // sPack, sView
+  b += (size_t)vmax * as * 4;        // sVal
+  b += 2 * 8 * 128 * 4;              // sRed
+  b += 2 * (size_t)zmax * zovl * 4;  // sTh
+  b += 9 * (size_t)(zmax + 2) * 4;   // sNb
+  b += 2 * (size_t)zmax * 4;         // sTn
+  b += (size_t)zmax * 4;             // sDelta
+  return b;
+}
+
+typedef void (*IcdKernel)(DevGeo, IcdArgs, int, int);
+
+// slot count: 4 covers delta_xy <= 1.5 delta_r, 12 covers delta_xy <= 4 delta_r
+static IcdKernel icd_kernel(int vec, int amode, int seq, int as) {
+#define XTG_K(V, M, S) (as == 4 ? k_icd_columns<V, M, S, 4> : k_icd_columns<V, M, S, 12>)
+  if (vec == 4) {
+    if (amode == 0) return seq ? XTG_K(4, 0, 1) : XTG_K(4, 0, 0);
+    return seq ? XTG_K(4, 1, 1) : XTG_K(4, 1, 0);
+  }
+  if (amode == 0) return seq ? XTG_K(1, 0, 1) : XTG_K(1, 0, 0);
+  return seq ? XTG_K(1, 1, 1) : XTG_K(1, 1, 0);
+#undef XTG_K
+}
+
+cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
+                       int grid, cudaStream_t st) {
+  const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as);
+  IcdKernel k = icd_kernel(vec, amode, seq, as);
+  cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, XTG_THREADS, smem, st>>>(G, A, vmax, zmax);
+  return cudaGetLastError();
+}
+
+int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl) {
+  const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as);
+  IcdKernel k = icd_kernel(vec, amode, seq, as);
+  int nb = 0;
+  cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)k, XTG_THREADS, smem) != cudaSuccess) return 1;
+  return nb > 0 ? nb : 1;
+}
+
+}  // namespace xtg

@@ -1,0 +1,29 @@
+/*
+ * xt_cli.h -- the XT_Engine command line.
+ *
+ * Same long options, short letters and defaults as the reference's
+ * argsParser (Source_Code_4D_Fast/XT_Init.c:452-629), so the launcher's
+ * command string (4D_Recon_Launcher_for_Real_Data/XT_MBIR_Reconstruction.py:124-157)
+ * runs unchanged.  A few long-only options (values >= 300) select what the
+ * reference fixes at compile time or what only the GPU engine has.
+ */
+#ifndef XT_CLI_H
+#define XT_CLI_H
+#include <stdint.h>
+
+#include "xt_geom.h"
+
+typedef struct {
+  int32_t a_fp16;       /* --gpu_afp16: FP16 A-matrix storage */
+  int32_t sequential;   /* --gpu_sequential: reference visiting order, one column at a time */
+  int32_t columns;      /* --gpu_columns N: columns in flight (0 = device default) */
+  uint64_t seed;        /* --gpu_seed S: seed of the GPU visiting order */
+  int32_t resync_every; /* --gpu_resync K: FP64 resync of e every K iterations (cost is FP64 every iteration) */
+  int32_t quiet;        /* --quiet: no stdout chatter */
+  int32_t n_unknown;    /* unrecognised options seen (reported, not fatal, like the reference) */
+} xt_engine_opts;
+
+/* Parses argv into *p and *o; returns 0, or 1 after printing usage for --help. */
+int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o);
+
+#endif
