@@ -90,6 +90,13 @@ int xtg_get_hr(const xtg_ctx *ctx, float *hr /*[N_p][65]*/);
 /* Options: A storage, update order, concurrent columns (0 = device default),
  * seed of the GPU visiting order. */
 int xtg_set_options(xtg_ctx *ctx, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed);
+/* Forward projections (xtg_forward_project, xtg_init_error_sino, the FP64
+ * resync and cost) either sum every sinogram entry over columns in the
+ * reference's (row, column) order -- exact = 1, FP32 results bit-identical
+ * to initErrorSinogam -- or accumulate in shared memory in any order --
+ * exact = 0, the default, about an order of magnitude faster and equal to
+ * the exact result up to FP32 rounding. */
+int xtg_set_exact_projection(xtg_ctx *ctx, int32_t exact);
 
 /* genSinogram_fromBin + computeWriteSinogram (XT_genSinogram.c:264-300,
  * XT_Engine.c:89-121): y, w and the offset d (NULL = zero).  Weights are

@@ -72,22 +72,45 @@ def test_amatrix_exhaustive_plain3d():
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_forward_projection_bit_exact(name):
     c, g, _ = ctx_for(name)
+    c.set_exact_projection(True)
     c.upload_object(g["x_true"])
     assert np.array_equal(c.forward_project(), g["ax"])
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
+def test_forward_projection_fast(name):
+    """Shared-memory accumulation in any order: within 1e-5 of the reference
+    projection relative to its largest value."""
+    c, g, _ = ctx_for(name)
+    c.upload_object(g["x_true"])
+    ax = c.forward_project()
+    scale = float(np.abs(g["ax"]).max())
+    assert np.max(np.abs(ax - g["ax"])) <= 1e-5 * scale
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
 def test_error_sinogram_and_cost(name):
     c, g, _ = ctx_for(name)
+    c.set_exact_projection(True)
     c.upload_sino(g["y"], g["w"])
     c.upload_object(g["x_true"])
     c.init_error_sino()
     assert np.array_equal(c.error_sino(), g["e_true"])
     cost, fwd, prior = c.cost()
+    # the reference sums its cost in FP32 (~1e-5 relative rounding over a few
+    # thousand terms); the GPU sums in FP64
     ref = g["cost_true"]
-    assert cost == pytest.approx(float(ref[0]), rel=1e-5)
-    assert fwd == pytest.approx(float(ref[1]), rel=1e-5)
-    assert prior == pytest.approx(float(ref[2]), rel=1e-5, abs=1e-6)
+    assert cost == pytest.approx(float(ref[0]), rel=1e-4)
+    assert fwd == pytest.approx(float(ref[1]), rel=1e-4)
+    assert prior == pytest.approx(float(ref[2]), rel=1e-4, abs=1e-6)
+    # against the FP64 oracle on the same object: the GPU evaluates in FP64
+    # with the FP32 build's prior constants (filter weights, sigma powers), so
+    # the two agree to FP32 rounding of those constants
+    o = Oracle(common.params(**CASES[name]), g["times"], g["angles"], double=True)
+    o.set_sino(g["y"], g["w"])
+    o.set_object(g["x_true"])
+    o.init_error_sino()
+    assert prior == pytest.approx(o.cost()[2], rel=1e-6, abs=1e-9)
     # the running-e cost and the FP64 resync agree with the recomputed cost
     assert c.cost_running()[0] == pytest.approx(cost, rel=1e-6)
     assert c.resync_fp64()[0] == pytest.approx(cost, rel=1e-12)
@@ -163,7 +186,11 @@ def test_parallel_icd_converges_to_oracle(name, amode):
     assert costs[-1] <= cstar * (1 + 1e-4), (costs[-1], cstar)
     x = c.object()
     rmse = float(np.sqrt(np.mean((x - xstar) ** 2)))
-    assert rmse / float(np.abs(xstar).max()) < 2e-2
+    # With zinger correction the generalized-Huber data term is not convex, so
+    # a different update order may settle in another minimum of equal cost;
+    # the RMSE bound is looser there.
+    bound = 1e-1 if CASES[name].get("zinger") else 2e-2
+    assert rmse / float(np.abs(xstar).max()) < bound
 
 
 def test_update_columns_list_api():

@@ -73,7 +73,7 @@ struct xtg_ctx {
   float *d_a16s = nullptr;
   int a16_vmax = 0, a16_ok = 0;
   // options
-  int a_mode = XTG_A_FP32, order = XTG_ORDER_PARALLEL, max_columns = 0;
+  int a_mode = XTG_A_FP32, order = XTG_ORDER_PARALLEL, max_columns = 0, exact_fp = 0;
   unsigned long long seed = 0x5eed5eedULL;
   int sm_count = 0;
   cudaStream_t st = nullptr;
@@ -258,6 +258,94 @@ __global__ void __launch_bounds__(256) k_fp(DevGeo G, FpArgs F) {
   }
 }
 
+// Fast forward projection: one CTA per (view, block of detector rows) holds
+// that view's sinogram rows in shared memory.  Each warp takes 32 columns at
+// a time, every lane evaluates the exact A entries of one column, then the
+// warp walks those 32 columns with lanes over detector rows, loading each
+// column's z-line once and adding x*A into the shared accumulator
+// (shared-memory atomics; the summation order is not the reference's, so
+// results agree with the exact gather to FP32 rounding).  z-lines that are
+// all zero are skipped.
+// MODE 0: ax; 1: e = y - Ax - d (FP32); 2: e from FP64 sums + data cost; 3: cost only.
+template <int MODE, typename ACC, int NS>
+__global__ void __launch_bounds__(512) k_fp_fast(DevGeo G, FpArgs F, int tc) {
+  extern __shared__ __align__(16) unsigned char fp_smem[];
+  ACC *acc = reinterpret_cast<ACC *>(fp_smem);  // [N_r][tc]
+  const int p = blockIdx.x, t0 = blockIdx.y * tc;
+  const int nt = min(tc, G.N_t - t0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int i = threadIdx.x; i < G.N_r * tc; i += blockDim.x) acc[i] = (ACC)0;
+  __syncthreads();
+  const int fr = F.fov[p];
+  const float cp = F.cosv[p], sp = F.sinv[p];
+  const float *H = F.hr + (size_t)p * XT_HR_STRIDE;
+  const int ncol = G.N_y * G.N_x;
+  for (int base = warp * 32; base < ncol; base += nwarp * 32) {
+    const int q = base + lane;
+    float vals[NS];
+    int first = 0, n = 0;
+    if (q < ncol) n = xt_amatrix_regs<NS>(G, H, cp, sp, q / G.N_x, q % G.N_x, vals, &first);
+    // columns in groups of 8: the 8 z-line loads are issued before any is
+    // used, so their L2 latencies overlap
+    for (int tb = 0; tb < nt; tb += 32) {
+      const int t = tb + lane;
+      for (int l0 = 0; l0 < 32; l0 += 8) {
+        float xv[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int ql = base + l0 + u;
+          xv[u] = (t < nt && ql < ncol) ? __ldg(F.x + ((size_t)fr * ncol + ql) * G.N_z + (t0 + t) / G.zovl) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int l = l0 + u;
+          const int nl = __shfl_sync(0xffffffffu, n, l);
+          if (nl == 0 || __ballot_sync(0xffffffffu, xv[u] != 0.f) == 0) continue;
+          const int fl = __shfl_sync(0xffffffffu, first, l);
+#pragma unroll
+          for (int s = 0; s < NS; s++) {
+            if (s < nl) {
+              const float a = __shfl_sync(0xffffffffu, vals[s], l);
+              if (xv[u] != 0.f && a != 0.f) atomicAdd(&acc[(fl + s) * tc + t], (ACC)xv[u] * (ACC)a);
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double cacc = 0.0;
+  for (int i = threadIdx.x; i < G.N_r * nt; i += blockDim.x) {
+    const int r = i / nt, t = i - r * nt;
+    const size_t o = ((size_t)p * G.N_r + r) * G.N_t + t0 + t;
+    const ACC s = acc[r * tc + t];
+    if (MODE == 0) {
+      F.out[o] = (float)s;
+    } else if (MODE == 1) {
+      F.out[o] = __fsub_rn(__fsub_rn(F.y[o], (float)s), F.d[(size_t)r * G.N_t + t0 + t]);
+    } else {
+      const double e64 = (double)F.y[o] - (double)s - (double)F.d[(size_t)r * G.N_t + t0 + t];
+      if (MODE == 2) F.out[o] = (float)e64;
+      const double sw = e64 * sqrt((double)F.w[o]);
+      if (fabs(sw) < (double)F.T)
+        cacc += sw * sw;
+      else
+        cacc += 2.0 * (double)F.delta * (double)F.T * fabs(sw) + (double)F.T * (double)F.T * (1.0 - 2.0 * (double)F.delta);
+    }
+  }
+  if (MODE >= 2) {
+    __shared__ double red[16];
+    for (int off = 16; off > 0; off >>= 1) cacc += __shfl_xor_sync(0xffffffffu, cacc, off);
+    if (lane == 0) red[warp] = cacc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0;
+      for (int w = 0; w < nwarp; w++) s += red[w];
+      atomicAdd(&F.cost_slots[(blockIdx.x + blockIdx.y * gridDim.x) % NSLOT], s);
+    }
+  }
+}
+
 // qGGMRF prior over forward neighbour pairs (XT_ICD_update.c:202-294), FP64.
 __global__ void k_prior_cost64(DevGeo G, const float *x, double *slots) {
   const size_t n = (size_t)G.N_time * G.N_y * G.N_x * G.N_z;
@@ -395,13 +483,21 @@ __global__ void __launch_bounds__(1024) k_radix_select(const float *vals, int se
 // columns above the threshold -> NHICD work items.  List 0 holds the
 // (frame, block) pairs the reference updates in its first half-pass (block
 // parity = frame parity, XT_ICD_update.c:846-857), list 1 the others.
-__global__ void k_nhicd_compact(int ntime, int nzb, int ny, int nx, const float *filt, const float *thr, int4 *list0,
-                                int4 *list1, int *cnt, int cap0, int cap1) {
+// A selected column outside the object-support disk has no voxel to update;
+// the reference still visits it, which only zeroes its MagUpdateMap entry
+// (XT_VoxUpdate.c:128, 138), so that is all done for it here.
+__global__ void k_nhicd_compact(int ntime, int nzb, int ny, int nx, const float *filt, const float *thr,
+                                const int *col_rank, float *mag, int4 *list0, int4 *list1, int *cnt, int cap0,
+                                int cap1) {
   const size_t n = (size_t)ntime * nzb * ny * nx;
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
     const size_t seg = q / ((size_t)nx * ny);
     if (!(filt[q] > thr[seg])) continue;
     const int k = (int)(q % nx), j = (int)((q / nx) % ny);
+    if (col_rank[(size_t)j * nx + k] < 0) {
+      mag[q] = 0.f;
+      continue;
+    }
     const int b = (int)(seg % nzb), f = (int)(seg / nzb);
     const int h = ((f & 1) == (b & 1)) ? 0 : 1;
     const int slot = atomicAdd(&cnt[h], 1);
@@ -656,16 +752,36 @@ static cudaError_t launch_fp(xtg_ctx *c, float *out, double *slots) {
   F.x = c->d_x; F.y = c->d_y; F.d = c->d_d; F.w = c->d_w; F.hr = c->d_hr; F.cosv = c->d_cos; F.sinv = c->d_sin;
   F.fov = c->d_fov; F.out = out; F.cost_slots = slots; F.T = c->g.T; F.delta = c->g.delta;
   F.win_margin = 1e-4 * (double)c->g.N_r * c->g.delta_r + 1e-3 * c->g.delta_r;
-  const long long warps = (long long)c->g.N_p * c->g.N_r;
-  const unsigned grid = (unsigned)((warps + 7) / 8);
-  const int vf = std::min(4, std::max(1, (c->g.N_t + 31) / 32));
-  if (vf == 1)
-    k_fp<MODE, 1><<<grid, 256, 0, c->st>>>(c->G, F);
-  else if (vf == 2)
-    k_fp<MODE, 2><<<grid, 256, 0, c->st>>>(c->G, F);
-  else
-    k_fp<MODE, 4><<<grid, 256, 0, c->st>>>(c->G, F);
   c->launches++;
+  if (c->exact_fp) {
+    // gather in the reference's summation order: FP32 results are bit-identical
+    const long long warps = (long long)c->g.N_p * c->g.N_r;
+    const unsigned grid = (unsigned)((warps + 7) / 8);
+    const int vf = std::min(4, std::max(1, (c->g.N_t + 31) / 32));
+    if (vf == 1)
+      k_fp<MODE, 1><<<grid, 256, 0, c->st>>>(c->G, F);
+    else if (vf == 2)
+      k_fp<MODE, 2><<<grid, 256, 0, c->st>>>(c->G, F);
+    else
+      k_fp<MODE, 4><<<grid, 256, 0, c->st>>>(c->G, F);
+    return cudaGetLastError();
+  }
+  const size_t esz = (MODE >= 2) ? sizeof(double) : sizeof(float);
+  const size_t budget = 200 * 1024;
+  int tc = (int)std::min<size_t>((size_t)c->g.N_t, budget / ((size_t)c->g.N_r * esz));
+  if (tc < 1) tc = 1;
+  const size_t smem = (size_t)c->g.N_r * tc * esz;
+  dim3 grid((unsigned)c->g.N_p, (unsigned)((c->g.N_t + tc - 1) / tc));
+  const int span = (int)ceil(2.0 * c->g.delta_xy / c->g.delta_r) + 1;
+  typedef void (*FpK)(DevGeo, FpArgs, int);
+  FpK k;
+  if (MODE >= 2)
+    k = span <= 3 ? k_fp_fast<MODE, double, 3> : span <= 4 ? k_fp_fast<MODE, double, 4> : k_fp_fast<MODE, double, 12>;
+  else
+    k = span <= 3 ? k_fp_fast<MODE, float, 3> : span <= 4 ? k_fp_fast<MODE, float, 4> : k_fp_fast<MODE, float, 12>;
+  cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, 512, smem, c->st>>>(c->G, F, tc);
   return cudaGetLastError();
 }
 
@@ -840,6 +956,12 @@ int xtg_set_options(xtg_ctx *c, int32_t a_mode, int32_t order, int32_t max_colum
   c->order = order;
   c->max_columns = max_columns;
   c->seed = seed;
+  return 0;
+}
+
+int xtg_set_exact_projection(xtg_ctx *c, int32_t exact) {
+  if (!c) return XTG_E_ARG;
+  c->exact_fp = exact ? 1 : 0;
   return 0;
 }
 
@@ -1150,25 +1272,29 @@ static int ensure_a16(xtg_ctx *c) {
 
 // one ICD launch over items[lo, lo+n) (or a device-counted list)
 static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, const int *n_dev, int use_perm,
-                       unsigned long long key, int whole_lines, int seq_override) {
+                       unsigned long long key, int has_whole, int has_blocks, int seq_override) {
   const xt_geom &g = c->g;
   if (c->a_mode == XTG_A_FP16) {
     int rc = ensure_a16(c);
     if (rc) return rc;
   }
   const int seq = (seq_override >= 0) ? seq_override : (c->order == XTG_ORDER_SEQUENTIAL);
-  // rows of one work item: a whole z-line, or one z-block (the last block is the longest)
-  const int zmax = whole_lines ? g.N_z : (g.N_z - (g.nzb - 1) * g.zstep);
+  // rows of the largest work item: a whole z-line, or one z-block (the last
+  // block is the longest); shared memory is sized for it
+  const int last_block = g.N_z - (g.nzb - 1) * g.zstep;
+  const int zmax = has_whole ? g.N_z : last_block;
   const int rows = zmax * g.zovl;
+  // 16-byte vector access needs every item's first row and row count to be
+  // multiples of 4 (the last block's rows too)
   bool v4 = (g.N_t % 4 == 0);
-  if (!whole_lines) v4 = v4 && ((g.zstep * g.zovl) % 4 == 0) && (rows % 4 == 0);
+  if (has_blocks) v4 = v4 && ((g.zstep * g.zovl) % 4 == 0) && ((last_block * g.zovl) % 4 == 0);
   const int vec = v4 ? 4 : 1;
   if ((rows + vec - 1) / vec > 32) {
     set_err("ICD work item of %d detector rows exceeds the kernel's %d (N_z/nzb too large)", rows, 32 * vec);
     return XTG_E_ARG;
   }
   const int span = (int)ceil(2.0 * g.delta_xy / g.delta_r) + 1;
-  const int as = span <= 4 ? 4 : 12;
+  const int as = span <= 3 ? 3 : span <= 4 ? 4 : 12;
   if (span > 12) {
     set_err("delta_xy too large for the ICD kernel (%d bins per view)", span);
     return XTG_E_ARG;
@@ -1217,8 +1343,8 @@ static int nhicd_select_device(xtg_ctx *c) {
   k_radix_select<<<nseg, 1024, 0, c->st>>>(c->d_filt, (int)c->nxy, c->d_kth, c->d_thr);
   CK(cudaMemsetAsync(c->d_nhcnt, 0, 8, c->st));
   const int cap0 = (int)(c->nh_cap / 2), cap1 = (int)(c->nh_cap - c->nh_cap / 2);
-  k_nhicd_compact<<<grid, 256, 0, c->st>>>(g.N_time, g.nzb, g.N_y, g.N_x, c->d_filt, c->d_thr, c->d_nh,
-                                           c->d_nh + cap0, c->d_nhcnt, cap0, cap1);
+  k_nhicd_compact<<<grid, 256, 0, c->st>>>(g.N_time, g.nzb, g.N_y, g.N_x, c->d_filt, c->d_thr, c->d_rank,
+                                           c->d_mag, c->d_nh, c->d_nh + cap0, c->d_nhcnt, cap0, cap1);
   k_clamp_count<<<1, 32, 0, c->st>>>(c->d_nhcnt, cap0, cap1);
   c->launches += 4;
   CK(cudaGetLastError());
@@ -1327,7 +1453,7 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
       if (rc) return rc;
     }
     CK(cudaEventRecord(c->ek0, c->st));
-    int rc = run_columns(c, iter, c->d_items, lo, hi - lo, nullptr, 0, 0, 1, -1);
+    int rc = run_columns(c, iter, c->d_items, lo, hi - lo, nullptr, 0, 0, 1, 0, -1);
     if (rc) return rc;
     CK(cudaEventRecord(c->ek1, c->st));
     if (j == K - 1) {
@@ -1350,7 +1476,7 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
     if (iter > 1 && !c->prm.no_NHICD) {
       for (int h = 0; h < 2; h++) {
         CK(cudaEventRecord(c->ek0, c->st));
-        rc = run_columns(c, iter, c->d_nh, h ? cap0 : 0, 0, c->d_nhcnt + h, 1, key + 17 * (j * 2 + h + 1), 0, -1);
+        rc = run_columns(c, iter, c->d_nh, h ? cap0 : 0, 0, c->d_nhcnt + h, 1, key + 17 * (j * 2 + h + 1), 0, 1, -1);
         if (rc) return rc;
         CK(cudaEventRecord(c->ek1, c->st));
         CK(cudaEventSynchronize(c->ek1));
@@ -1392,7 +1518,7 @@ static int icd_iteration_sequential(xtg_ctx *c, int iter, xtg_stats *st) {
     }
     CK(cudaMemcpyAsync(c->d_items, L.data(), L.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
     CK(cudaEventRecord(c->ek0, c->st));
-    int rc = run_columns(c, iter, c->d_items, 0, (int)L.size(), nullptr, 0, 0, 0, 1);
+    int rc = run_columns(c, iter, c->d_items, 0, (int)L.size(), nullptr, 0, 0, 0, 1, 1);
     if (rc) return rc;
     CK(cudaEventRecord(c->ek1, c->st));
     CK(cudaEventSynchronize(c->ek1));
@@ -1467,7 +1593,11 @@ static int icd_iteration_sequential(xtg_ctx *c, int iter, xtg_stats *st) {
           for (int b = 0; b < g.nzb; b += 2) {
             const int idx = (((i % 2) == 0) ^ half) ? b : b + 1;
             const int s = i * g.nzb + idx;
-            for (int q = 0; q < nsn[s]; q++) items.push_back(make_int4(i, yn[(size_t)s * nxy + q], xn[(size_t)s * nxy + q], idx));
+            for (int q = 0; q < nsn[s]; q++) {
+              const int yy = yn[(size_t)s * nxy + q], xx = xn[(size_t)s * nxy + q];
+              // a selected column outside the support disk has no voxel to update
+              if (c->col_rank[(size_t)yy * g.N_x + xx] >= 0) items.push_back(make_int4(i, yy, xx, idx));
+            }
           }
         int rc = run_list(items);
         if (rc) return rc;
@@ -1536,7 +1666,7 @@ int xtg_update_columns(xtg_ctx *c, int32_t iter, int32_t n, const int32_t *items
     return XTG_E_ARG;
   }
   const xt_geom &g = c->g;
-  int whole = 1;
+  int any_whole = 0, any_block = 0;
   for (int q = 0; q < n; q++) {
     const int f = items[4 * q], r = items[4 * q + 1], k = items[4 * q + 2], b = items[4 * q + 3];
     if (f < 0 || f >= g.N_time || r < 0 || r >= g.N_y || k < 0 || k >= g.N_x || b < -1 || b >= g.nzb) {
@@ -1547,7 +1677,7 @@ int xtg_update_columns(xtg_ctx *c, int32_t iter, int32_t n, const int32_t *items
       set_err("xtg_update_columns: FP16 A covers masked columns only (item %d)", q);
       return XTG_E_ARG;
     }
-    if (b >= 0) whole = 0;
+    if (b >= 0) any_block = 1; else any_whole = 1;
   }
   xtg_stats st;
   memset(&st, 0, sizeof(st));
@@ -1555,7 +1685,7 @@ int xtg_update_columns(xtg_ctx *c, int32_t iter, int32_t n, const int32_t *items
   if (rc) return rc;
   if (n) CK(cudaMemcpyAsync(c->d_items, items, (size_t)n * sizeof(int4), cudaMemcpyHostToDevice, c->st));
   CK(cudaEventRecord(c->ek0, c->st));
-  rc = run_columns(c, iter, c->d_items, 0, n, nullptr, 0, 0, whole, -1);
+  rc = run_columns(c, iter, c->d_items, 0, n, nullptr, 0, 0, any_whole, any_block, -1);
   if (rc) return rc;
   CK(cudaEventRecord(c->ek1, c->st));
   double ab = 0;

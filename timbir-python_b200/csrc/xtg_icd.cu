@@ -3,14 +3,15 @@
 //
 // Parallel-beam A is z-invariant: every slice of a column sees the same
 // (view, bin) entries, and the rows of slice z are t = z*zovl .. z*zovl+zovl-1.
-// So the CTA computes the column's A once into shared memory, then streams
-// the column's footprint e[p][bin][t0..t0+T) and w[...] (contiguous in t) with
-// vector loads, thread (view-group, t-lane) accumulating theta1/theta2 for its
-// rows; shuffles and a shared-memory pass reduce them over view groups.  The
-// slices' qGGMRF surrogate steps run in red/black z order (or strictly in
-// increasing z, the reference's order, in sequential mode), and the e update
-// goes back with vector red.global.add, so columns in flight that share
-// sinogram entries never lose an update.
+// So the CTA puts the column's A into shared memory once (computed in
+// registers, or read from the FP16 table), then streams the column's
+// footprint e[p][bin][t0..t0+T) and w[...] (contiguous in t) with 16-byte
+// loads, thread (view group, t lane) accumulating theta1/theta2 for its rows;
+// shuffles and one shared-memory pass reduce them over view groups.  The
+// slices' qGGMRF surrogate steps run in red/black z order with 8 lanes per
+// voxel (or strictly in increasing z on one thread, the reference's order, in
+// sequential mode), and the e update goes back with vector red.global.add,
+// so columns in flight that share sinogram entries never lose an update.
 //
 // Reference: updateVoxels_Aditya + compute_voxel_update_Aditya
 // (Source_Code_4D_Fast/XT_VoxUpdate.c:11-254), CE_FunctionalSubstitution
@@ -20,19 +21,55 @@
 
 namespace xtg {
 
+// surrogate coefficient with fast intrinsics: the step size only needs a few
+// digits, the fixed point of the iteration is unchanged
+__device__ __forceinline__ float qcoef_fast(float d, float sq, float sqp, float c, float p) {
+  if (d == 0.f) return __fdividef(2.0f, sq * c);
+  const float t1 = __fdividef(__powf(fabsf(d), 2.0f - p), sqp);
+  const float t3 = c + t1;
+  return __fdividef(2.0f - __fdividef((2.0f - p) * t1, t3), t3 * sq);
+}
+
+// the 29 neighbour slots of a voxel: 0..26 the 3x3x3 block in [dz][dy][dx]
+// order (13 = the voxel itself, skipped), 27 = frame - 1, 28 = frame + 1
+struct Nbr {
+  float v;
+  float b;  // filter weight * surrogate coefficient, 0 when the slot is absent
+};
+
+__device__ __forceinline__ Nbr nbr_term(const DevGeo &G, const float *sNb, const float *sTn, int zmax, int z, int zb,
+                                        int fr, int row, int col, float Vv, int n) {
+  Nbr o{0.f, 0.f};
+  if (n < 27) {
+    if (n == 13) return o;
+    const int dz = n / 9, c = n % 9;
+    const int za = zb + z + dz - 1;
+    if (za < 0 || za >= G.N_z) return o;
+    const int jj = row + c / 3 - 1, kk = col + c % 3 - 1;
+    if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x) return o;
+    o.v = sNb[c * (zmax + 2) + z + dz];
+    o.b = G.SF[n] * qcoef_fast(Vv - o.v, G.Sigma_S_Q, G.Sigma_S_Q_P, G.C_S, G.MRF_P);
+  } else {
+    const int f2 = fr + (n == 27 ? -1 : 1);
+    if (f2 < 0 || f2 >= G.N_time) return o;
+    o.v = sTn[(n - 27) * zmax + z];
+    o.b = G.TF * qcoef_fast(Vv - o.v, G.Sigma_T_Q, G.Sigma_T_Q_P, G.C_T, G.MRF_P);
+  }
+  return o;
+}
 
 template <int VEC, int AMODE, int SEQ, int AS>
-__global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArgs A, int vmax, int zmax) {
+__global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArgs A, int vmax, int zmax) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  int *sPack = reinterpret_cast<int *>(smem_raw);               // [vmax] first | cnt << 24
-  int *sView = sPack + vmax;                                     // [vmax] view index p
-  float *sVal = reinterpret_cast<float *>(sView + vmax);         // [vmax * AS] A * delta_t
-  float *sRed = sVal + (size_t)vmax * AS;                    // [2][8][128] warp partials
-  float *sTh = sRed + 2 * 8 * 128;                               // [2][zmax*zovl]
+  int *sPack = reinterpret_cast<int *>(smem_raw);        // [vmax] first | n << 24
+  int *sView = sPack + vmax;                              // [vmax] view index p
+  float *sVal = reinterpret_cast<float *>(sView + vmax);  // [AS][vmax] A * delta_t
+  float *sRed = sVal + (size_t)vmax * AS;                 // [2][8][128] warp partials
+  float *sTh = sRed + 2 * 8 * 128;                        // [2][zmax*zovl]
   const int rowsmax = zmax * G.zovl;
-  float *sNb = sTh + 2 * rowsmax;                                // [9][zmax+2]
-  float *sTn = sNb + 9 * (zmax + 2);                             // [2][zmax]
-  float *sDelta = sTn + 2 * zmax;                                // [zmax]
+  float *sNb = sTh + 2 * rowsmax;                         // [9][zmax+2]
+  float *sTn = sNb + 9 * (zmax + 2);                      // [2][zmax]
+  float *sDelta = sTn + 2 * zmax;                         // [zmax]
   __shared__ int sItem;
   __shared__ double sAbs[XTG_THREADS / 32];
   __shared__ unsigned sUpd, sZero;
@@ -64,13 +101,14 @@ __global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArg
     if (AMODE == 0) {
       for (int v = tid; v < V; v += XTG_THREADS) {
         const int p = A.view_idx[vs + v];
-        float vals[XT_AMAX];
+        float vals[AS];
         int first;
-        const int n = xt_amatrix_view(G, A.hr + (size_t)p * XT_HR_STRIDE, A.cosv[p], A.sinv[p], row, col, vals, &first);
-        sPack[v] = first | (min(n, AS) << 24);
+        const int n = xt_amatrix_regs<AS>(G, A.hr + (size_t)p * XT_HR_STRIDE, A.cosv[p], A.sinv[p], row, col, vals,
+                                          &first);
+        sPack[v] = first | (n << 24);
         sView[v] = p;
 #pragma unroll
-        for (int s = 0; s < AS; s++) sVal[v * AS + s] = (s < n) ? __fmul_rn(vals[s], G.delta_t) : 0.f;
+        for (int s = 0; s < AS; s++) sVal[s * vmax + v] = __fmul_rn(vals[s], G.delta_t);
       }
     } else {
       const int rk = A.col_rank[row * G.N_x + col];
@@ -83,10 +121,9 @@ __global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArg
         sView[v] = A.view_idx[vs + v];
         const __half2 h01 = *reinterpret_cast<const __half2 *>(&r4.y);
         const __half2 h23 = *reinterpret_cast<const __half2 *>(&r4.z);
-        sVal[v * AS + 0] = __low2float(h01) * sc;
-        sVal[v * AS + 1] = __high2float(h01) * sc;
-        sVal[v * AS + 2] = __low2float(h23) * sc;
-        sVal[v * AS + 3] = __high2float(h23) * sc;
+        const float hv[4] = {__low2float(h01), __high2float(h01), __low2float(h23), __high2float(h23)};
+#pragma unroll
+        for (int s = 0; s < AS; s++) sVal[s * vmax + v] = (s < 4) ? hv[s < 4 ? s : 0] * sc : 0.f;
       }
     }
     // 2. neighbourhood: the 3x3 columns' z-lines over [zb-1, ze+1], and the
@@ -124,7 +161,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArg
 #pragma unroll
         for (int s = 0; s < AS; s++) {
           if (s < n) {
-            const float a = sVal[v * AS + s];
+            const float a = sVal[s * vmax + v], a2 = a * a;
             float ev[VEC], wv[VEC];
             if (VEC == 4) {
               const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(A.e + base + (size_t)s * G.N_t));
@@ -138,14 +175,30 @@ __global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArg
                 wv[c] = __ldg(A.w + base + (size_t)s * G.N_t + c);
               }
             }
+            // generalized-Huber (zinger) weight: w where |e sqrt(w)| < T,
+            // else T delta sqrt(w) / |e| (XT_VoxUpdate.c:34-48); the slow
+            // branch runs only when some lane of the warp needs it
+            float ew[VEC];
+            bool zg = false;
 #pragma unroll
             for (int c = 0; c < VEC; c++) {
-              // generalized-Huber (zinger) weight: w where |e sqrt(w)| < T,
-              // else T delta sqrt(w)/|e| (XT_VoxUpdate.c:34-48)
-              float we = wv[c];
-              if (ev[c] * ev[c] * wv[c] >= A.T2) we = A.Tdelta * sqrtf(wv[c]) / fabsf(ev[c]);
-              th2[c] += a * a * we;
-              th1[c] -= ev[c] * a * we;
+              ew[c] = ev[c] * wv[c];
+              zg |= (ev[c] * ew[c] >= A.T2);
+            }
+            if (__any_sync(__activemask(), zg)) {
+#pragma unroll
+              for (int c = 0; c < VEC; c++) {
+                float we = wv[c];
+                if (ev[c] * ew[c] >= A.T2) we = __fdividef(A.Tdelta * sqrtf(wv[c]), fabsf(ev[c]));
+                th2[c] = fmaf(a2, we, th2[c]);
+                th1[c] = fmaf(-a * ev[c], we, th1[c]);
+              }
+            } else {
+#pragma unroll
+              for (int c = 0; c < VEC; c++) {
+                th2[c] = fmaf(a2, wv[c], th2[c]);
+                th1[c] = fmaf(-a, ew[c], th1[c]);
+              }
             }
           }
         }
@@ -169,6 +222,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArg
     __syncthreads();
     for (int t = tid; t < T; t += XTG_THREADS) {
       float s1 = 0.f, s2 = 0.f;
+#pragma unroll
       for (int wq = 0; wq < XTG_THREADS / 32; wq++) {  // every warp wrote its partial (zeros if idle)
         s1 += sRed[wq * 128 + t];
         s2 += sRed[8 * 128 + wq * 128 + t];
@@ -181,75 +235,115 @@ __global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArg
     // 4. qGGMRF surrogate step per slice (CE_FunctionalSubstitution,
     //    XT_ICD_update.c:130-179) with zero skipping (XT_VoxUpdate.c:208-232)
     double absx = 0.0;
-    auto update = [&](int z) {
-      const int zz = z + 1;
-      const float Vv = sNb[4 * (zmax + 2) + zz];
-      float t1 = 0.f, t2 = 0.f;
-      for (int r = 0; r < G.zovl; r++) {
-        t1 += sTh[z * G.zovl + r];
-        t2 += sTh[rowsmax + z * G.zovl + r];
-      }
-      const int za = zb + z;
-      const bool zdn = za - 1 >= 0, zup = za + 1 < G.N_z;
-      const bool tdn = fr - 1 >= 0, tup = fr + 1 < G.N_time;
-      if (Vv == 0.f && A.iter > 1) {
-        bool skip = !(sTn[z] > 0.f || sTn[zmax + z] > 0.f);
-        for (int c = 0; c < 9 && skip; c++)
-          for (int dz = 0; dz < 3; dz++)
-            if (sNb[c * (zmax + 2) + zz - 1 + dz] > 0.f) skip = false;
-        if (skip) {
-          sDelta[z] = 0.f;
-          atomicAdd(&sZero, 1u);
-          return;
-        }
-      }
-      float num = 0.f, den = 0.f;
-#pragma unroll
-      for (int dz = 0; dz < 3; dz++) {
-        if ((dz == 0 && !zdn) || (dz == 2 && !zup)) continue;
-#pragma unroll
-        for (int c = 0; c < 9; c++) {
-          if (dz == 1 && c == 4) continue;
-          const int jj = row + c / 3 - 1, kk = col + c % 3 - 1;
-          if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x) continue;
-          const float nv = sNb[c * (zmax + 2) + zz - 1 + dz];
-          const float b = G.SF[dz * 9 + c] * xt_qggmrf_coef(Vv - nv, G.Sigma_S_Q, G.Sigma_S_Q_P, G.C_S, G.MRF_P);
-          num += b * nv;
-          den += b;
-        }
-      }
-      if (tdn) {
-        const float nv = sTn[z];
-        const float b = G.TF * xt_qggmrf_coef(Vv - nv, G.Sigma_T_Q, G.Sigma_T_Q_P, G.C_T, G.MRF_P);
-        num += b * nv;
-        den += b;
-      }
-      if (tup) {
-        const float nv = sTn[zmax + z];
-        const float b = G.TF * xt_qggmrf_coef(Vv - nv, G.Sigma_T_Q, G.Sigma_T_Q_P, G.C_T, G.MRF_P);
-        num += b * nv;
-        den += b;
-      }
-      const float u = (num + t2 * Vv - t1) / (den + t2);
-      float nvx = Vv + G.alpha * (u - Vv);
-      if (G.positivity && nvx <= 0.f) nvx = 0.f;
-      if (!isfinite(nvx)) {
-        atomicExch(A.err, 1);
-        nvx = Vv;
-      }
-      sNb[4 * (zmax + 2) + zz] = nvx;
-      A.x[(((size_t)fr * plane) + (size_t)row * G.N_x + col) * G.N_z + za] = nvx;
-      sDelta[z] = nvx - Vv;
-      absx += (double)fabsf(nvx);
-      atomicAdd(&sUpd, 1u);
-    };
     if (SEQ) {
-      if (tid == 0)
-        for (int z = 0; z < Z; z++) update(z);
+      if (tid == 0) {
+        for (int z = 0; z < Z; z++) {
+          const float Vv = sNb[4 * (zmax + 2) + z + 1];
+          float t1 = 0.f, t2 = 0.f;
+          for (int r = 0; r < G.zovl; r++) {
+            t1 += sTh[z * G.zovl + r];
+            t2 += sTh[rowsmax + z * G.zovl + r];
+          }
+          bool skip = false;
+          if (Vv == 0.f && A.iter > 1) {
+            skip = !(sTn[z] > 0.f || sTn[zmax + z] > 0.f);
+            for (int c = 0; c < 9 && skip; c++)
+              for (int dz = 0; dz < 3; dz++)
+                if (sNb[c * (zmax + 2) + z + dz] > 0.f) skip = false;
+          }
+          if (skip) {
+            sDelta[z] = 0.f;
+            sZero++;
+            continue;
+          }
+          float num = 0.f, den = 0.f;
+          for (int n = 0; n < 29; n++) {
+            const Nbr o = nbr_term(G, sNb, sTn, zmax, z, zb, fr, row, col, Vv, n);
+            num += o.b * o.v;
+            den += o.b;
+          }
+          const float u = (num + t2 * Vv - t1) / (den + t2);
+          float nvx = Vv + G.alpha * (u - Vv);
+          if (G.positivity && nvx <= 0.f) nvx = 0.f;
+          if (!isfinite(nvx)) {
+            atomicExch(A.err, 1);
+            nvx = Vv;
+          }
+          sNb[4 * (zmax + 2) + z + 1] = nvx;
+          A.x[(((size_t)fr * plane) + (size_t)row * G.N_x + col) * G.N_z + zb + z] = nvx;
+          sDelta[z] = nvx - Vv;
+          absx += (double)fabsf(nvx);
+          sUpd++;
+        }
+      }
     } else {
+      // red/black in z, 8 lanes per voxel, each lane a subset of the 29
+      // neighbour slots; the lane group reduces with shuffles
+      const int sub = tid & 7, slot = tid >> 3;
       for (int par = 0; par < 2; par++) {
-        for (int z = tid; z < Z; z += XTG_THREADS)
-          if (((zb + z) & 1) == par) update(z);
+        const int zfirst = ((zb & 1) == par) ? 0 : 1;  // first z (relative) with absolute parity par
+        const int nvox = (Z - zfirst + 1) / 2;
+        for (int s0 = 0; s0 < nvox; s0 += XTG_THREADS / 8) {
+          const int vi = s0 + slot;
+          const bool act = vi < nvox;
+          const int z = zfirst + 2 * (act ? vi : 0);
+          const float Vv = sNb[4 * (zmax + 2) + z + 1];
+          // zero skipping: V == 0 from the second iteration and no positive neighbour
+          bool pos = false;
+          float num = 0.f, den = 0.f;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const int n = sub + 8 * k;
+            if (n < 29) {
+              const Nbr o = nbr_term(G, sNb, sTn, zmax, z, zb, fr, row, col, Vv, n);
+              num += o.b * o.v;
+              den += o.b;
+            }
+          }
+          // positive-neighbour test over the raw values (absent slots read 0)
+          if (Vv == 0.f && A.iter > 1) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const int n = sub + 8 * k;
+              if (n < 27) {
+                if (sNb[(n % 9) * (zmax + 2) + z + n / 9] > 0.f) pos = true;
+              } else if (n < 29) {
+                if (sTn[(n - 27) * zmax + z] > 0.f) pos = true;
+              }
+            }
+          }
+#pragma unroll
+          for (int off = 1; off < 8; off <<= 1) {
+            num += __shfl_xor_sync(0xffffffffu, num, off);
+            den += __shfl_xor_sync(0xffffffffu, den, off);
+            pos |= __shfl_xor_sync(0xffffffffu, (int)pos, off) != 0;
+          }
+          if (act && sub == 0) {
+            const int zr = z;
+            if (Vv == 0.f && A.iter > 1 && !pos) {
+              sDelta[zr] = 0.f;
+              atomicAdd(&sZero, 1u);
+            } else {
+              float t1 = 0.f, t2 = 0.f;
+              for (int r = 0; r < G.zovl; r++) {
+                t1 += sTh[zr * G.zovl + r];
+                t2 += sTh[rowsmax + zr * G.zovl + r];
+              }
+              const float u = (num + t2 * Vv - t1) / (den + t2);
+              float nvx = Vv + G.alpha * (u - Vv);
+              if (G.positivity && nvx <= 0.f) nvx = 0.f;
+              if (!isfinite(nvx)) {
+                atomicExch(A.err, 1);
+                nvx = Vv;
+              }
+              sNb[4 * (zmax + 2) + zr + 1] = nvx;
+              A.x[(((size_t)fr * plane) + (size_t)row * G.N_x + col) * G.N_z + zb + zr] = nvx;
+              sDelta[zr] = nvx - Vv;
+              absx += (double)fabsf(nvx);
+              atomicAdd(&sUpd, 1u);
+            }
+          }
+        }
         __syncthreads();
       }
     }
@@ -295,7 +389,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 2) k_icd_columns(DevGeo G, IcdArg
 #pragma unroll
           for (int s = 0; s < AS; s++) {
             if (s < n) {
-              const float a = sVal[v * AS + s];
+              const float a = sVal[s * vmax + v];
               if (VEC == 4) {
                 xt_red_add4(ep + (size_t)s * G.N_t, -(a * dv[0]), -(a * dv[1]), -(a * dv[2]), -(a * dv[3]));
               } else {
@@ -326,9 +420,10 @@ size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as) {
 
 typedef void (*IcdKernel)(DevGeo, IcdArgs, int, int);
 
-// slot count: 4 covers delta_xy <= 1.5 delta_r, 12 covers delta_xy <= 4 delta_r
+// slot count: 3 covers delta_xy <= delta_r, 4 covers delta_xy <= 1.5 delta_r,
+// 12 covers delta_xy <= 5.5 delta_r
 static IcdKernel icd_kernel(int vec, int amode, int seq, int as) {
-#define XTG_K(V, M, S) (as == 4 ? k_icd_columns<V, M, S, 4> : k_icd_columns<V, M, S, 12>)
+#define XTG_K(V, M, S) (as == 3 ? k_icd_columns<V, M, S, 3> : as == 4 ? k_icd_columns<V, M, S, 4> : k_icd_columns<V, M, S, 12>)
   if (vec == 4) {
     if (amode == 0) return seq ? XTG_K(4, 0, 1) : XTG_K(4, 0, 0);
     return seq ? XTG_K(4, 1, 1) : XTG_K(4, 1, 0);
@@ -344,6 +439,11 @@ cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, in
   IcdKernel k = icd_kernel(vec, amode, seq, as);
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  // e and w stream through L2 (e must, it is updated by other CTAs' atomics),
+  // so give the unified L1/shared space to shared memory: more CTAs per SM
+  e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
   k<<<grid, XTG_THREADS, smem, st>>>(G, A, vmax, zmax);
   return cudaGetLastError();
 }
@@ -353,6 +453,8 @@ int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int z
   IcdKernel k = icd_kernel(vec, amode, seq, as);
   int nb = 0;
   cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute((const void *)k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)k, XTG_THREADS, smem) != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }

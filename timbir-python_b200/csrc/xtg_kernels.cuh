@@ -76,6 +76,66 @@ __device__ __forceinline__ int xt_amatrix_view(const DevGeo &G, const float *__r
   return n;
 }
 
+// Register-only form of xt_amatrix_view for at most NS kept bins: slot q holds
+// bin imin + q, then leading empty slots are shifted out, so every array
+// index is a compile-time constant (no local memory).  Same values as the
+// reference's calcAMatrixColumnforAngle.
+template <int NS>
+__device__ __forceinline__ int xt_amatrix_regs(const DevGeo &G, const float *__restrict__ H, float cp, float sp,
+                                               int row, int col, float (&v)[NS], int *first) {
+  constexpr int QM = NS + 2;  // imax - imin + 1 never exceeds NS + 2 (floor rounding of +-delta_xy)
+  float f[QM];
+#pragma unroll
+  for (int q = 0; q < QM; q++) f[q] = 0.f;
+  *first = 0;
+  const float x = xt_coord(G.x0, col, G.delta_xy);
+  const float y = xt_coord(G.y0, row, G.delta_xy);
+  const float r = __fsub_rn(__fmul_rn(x, cp), __fmul_rn(y, sp));
+  const float rmin = __fsub_rn(r, G.delta_xy), rmax = __fadd_rn(r, G.delta_xy);
+  int imin = 0;
+  if (!(rmax < G.R0 || rmin > G.RMax)) {
+    imin = (int)floorf(__fdiv_rn(__fsub_rn(rmin, G.R0), G.delta_r));
+    int imax = (int)floorf(__fdiv_rn(__fsub_rn(rmax, G.R0), G.delta_r));
+    if (imax >= G.N_r) imax = G.N_r - 1;
+    if (imin < 0) imin = 0;
+#pragma unroll
+    for (int q = 0; q < QM; q++) {
+      const int j = imin + q;
+      if (j <= imax) {
+        const float rc = xt_coord(G.R0, j, G.delta_r);
+        const float dr = fabsf(__fsub_rn(r, rc));
+        const int id = (int)floorf(__fdiv_rn(dr, G.OffsetR));
+        if (id >= 0 && id < XT_HR_BINS) {
+          const float w1 = __fsub_rn(dr, __fmul_rn((float)id, G.OffsetR));
+          const float w2 = __fsub_rn(G.OffsetR, w1);
+          const float f1 = __fdiv_rn(__fadd_rn(__fmul_rn(w2, H[id]), __fmul_rn(w1, H[id + 1])), G.OffsetR);
+          if (f1 > 0.f) f[q] = f1;
+        }
+      }
+    }
+  }
+  // shift leading empty slots out (bounded, constant indices)
+  int lead = 0;
+#pragma unroll
+  for (int it = 0; it < QM - 1; it++) {
+    if (f[0] == 0.f && lead < QM - 1) {
+#pragma unroll
+      for (int q = 0; q < QM - 1; q++) f[q] = f[q + 1];
+      f[QM - 1] = 0.f;
+      lead++;
+    }
+  }
+  int n = 0;
+#pragma unroll
+  for (int q = 0; q < QM; q++)
+    if (f[q] > 0.f) n = q + 1;
+  if (n > NS) n = NS;  // cannot happen: the reference's own buffer holds ceil(3 delta_xy / delta_r) entries
+#pragma unroll
+  for (int q = 0; q < NS; q++) v[q] = f[q];
+  *first = imin + lead;
+  return n;
+}
+
 // The single entry A[(view, bin), (row, col)], or 0 when the reference keeps
 // no entry for that bin.
 __device__ __forceinline__ float xt_amatrix_entry(const DevGeo &G, const float *__restrict__ H, float cp, float sp,
