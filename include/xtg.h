@@ -170,6 +170,30 @@ int xtg_nhicd_select(xtg_ctx *ctx, const int32_t *update_select_num, int32_t *nh
 int xtg_update_offset(xtg_ctx *ctx);
 int xtg_update_variance(xtg_ctx *ctx);
 
+/* NHICD thresholds without allocating any device memory.  No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc -- hosts
+ * that own every device buffer through their own pool and allow no
+ * allocation once started (for instance a beamline acquisition loop, where
+ * cudaMalloc's implicit device-wide synchronisation would stall the detector
+ * stream).  The caller passes device buffers: magmap [nmaps][ny][nx] (the
+ * magnitude-update maps), thresholds [nmaps] (out: for map s the kth[s]-th
+ * smallest value, 1-based, of its 5x5 Hamming-filtered map, as
+ * xtg_nhicd_select computes) and, when not NULL, select [nmaps][ny][nx] (out:
+ * 1 where the filtered value exceeds the threshold); kth is a host array.
+ * Work is queued on `stream` (a cudaStream_t, NULL = default stream) and is
+ * complete when that stream is.
+ * Scratch is one fixed array inside the library, XTG_NOALLOC_MAX_ELEMS floats
+ * (4 MiB) plus XTG_NOALLOC_MAX_MAPS ints, held on every GPU that loads the
+ * library until the process exits; larger inputs are rejected with XTG_E_ARG.
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race on it and must be serialised by the caller. */
+#define XTG_NOALLOC_MAX_ELEMS (1 << 20)
+#define XTG_NOALLOC_MAX_MAPS 256
+int xtg_nhicd_threshold_noalloc(const float *magmap, int32_t nmaps, int32_t ny, int32_t nx, const int32_t *kth,
+                                float *thresholds, uint8_t *select, void *stream);
+
 /* Device bytes held by the context. */
 int64_t xtg_device_bytes(const xtg_ctx *ctx);
 /* Kernel launches issued by this context since creation (all kernels). */

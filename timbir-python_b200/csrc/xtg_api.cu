@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1750,3 +1751,77 @@ int xtg_last_kernel_time(const xtg_ctx *c, float *ms, int64_t *items, int64_t *r
 }
 
 }  // extern "C"
+
+// ------------------------------------------- allocation-free NHICD threshold --
+// Scratch of xtg_nhicd_threshold_noalloc: the filtered maps, then the per-map
+// ranks.  It lives for the life of the library on every device that loads it.
+// Host code must not use the symbol itself as a device address (it is a host
+// stand-in); the device address comes from cudaGetSymbolAddress, once per
+// device.
+static __device__ __align__(256) float g_noalloc_scratch[XTG_NOALLOC_MAX_ELEMS + XTG_NOALLOC_MAX_MAPS];
+
+struct NoallocRanks {
+  int k[XTG_NOALLOC_MAX_MAPS];
+};
+
+// the ranks travel by value in the launch, so no host-to-device copy (and no
+// staging allocation) is needed
+__global__ void k_noalloc_put_ranks(NoallocRanks r, int n, int *dst) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = r.k[i];
+}
+
+__global__ void k_noalloc_select(size_t n, int plane, const float *filt, const float *thr, unsigned char *sel) {
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    sel[q] = filt[q] > thr[q / plane] ? 1 : 0;
+}
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_addr[256];
+
+extern "C" int xtg_nhicd_threshold_noalloc(const float *magmap, int32_t nmaps, int32_t ny, int32_t nx,
+                                           const int32_t *kth, float *thresholds, uint8_t *select, void *stream) {
+  if (!magmap || !kth || !thresholds || nmaps < 1 || ny < 1 || nx < 1) {
+    set_err("xtg_nhicd_threshold_noalloc: null pointer or empty map");
+    return XTG_E_ARG;
+  }
+  const size_t plane = (size_t)ny * nx, n = (size_t)nmaps * plane;
+  if (n > (size_t)XTG_NOALLOC_MAX_ELEMS || nmaps > XTG_NOALLOC_MAX_MAPS) {
+    set_err("xtg_nhicd_threshold_noalloc: %d maps of %d x %d (%zu values) exceed the fixed scratch of %d values "
+            "in at most %d maps; use xtg_nhicd_select instead",
+            nmaps, ny, nx, n, XTG_NOALLOC_MAX_ELEMS, XTG_NOALLOC_MAX_MAPS);
+    return XTG_E_ARG;
+  }
+  NoallocRanks r;
+  for (int s = 0; s < nmaps; s++) {
+    if (kth[s] < 1 || (size_t)kth[s] > plane) {
+      set_err("xtg_nhicd_threshold_noalloc: rank %d of map %d outside 1..%zu", kth[s], s, plane);
+      return XTG_E_ARG;
+    }
+    r.k[s] = kth[s];
+  }
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) {
+    set_err("xtg_nhicd_threshold_noalloc: device ordinal %d out of range", dev);
+    return XTG_E_ARG;
+  }
+  void *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {  // first call on this device: resolve the array's device address
+      CK(cudaGetSymbolAddress(&g_noalloc_addr[dev], g_noalloc_scratch));
+    }
+    base = g_noalloc_addr[dev];
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  float *filt = reinterpret_cast<float *>(base);
+  int *ranks = reinterpret_cast<int *>(filt + XTG_NOALLOC_MAX_ELEMS);
+  // every value read below is written first in this call: no clearing needed
+  k_noalloc_put_ranks<<<1, 256, 0, st>>>(r, nmaps, ranks);
+  const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, 4096);
+  k_vsc_filter<<<grid, 256, 0, st>>>(nmaps, ny, nx, magmap, filt);
+  k_radix_select<<<nmaps, 1024, 0, st>>>(filt, (int)plane, ranks, thresholds);
+  if (select) k_noalloc_select<<<grid, 256, 0, st>>>(n, (int)plane, filt, thresholds, select);
+  CK(cudaGetLastError());
+  return 0;
+}

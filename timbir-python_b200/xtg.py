@@ -33,6 +33,7 @@ XTG_SYMBOLS = [
     "xtg_resync_fp64", "xtg_map_cost_fp64", "xtg_map_cost_running", "xtg_zinger_refresh",
     "xtg_icd_iteration", "xtg_update_columns", "xtg_nhicd_select", "xtg_update_offset",
     "xtg_update_variance", "xtg_device_bytes", "xtg_launch_count", "xtg_last_kernel_time",
+    "xtg_nhicd_threshold_noalloc",
 ]
 XTGEN_SYMBOLS = [
     "xtgen_views_uniform", "xtgen_views_interlaced", "xtgen_write_view_file", "xtgen_phantom",
@@ -108,6 +109,8 @@ def gpu_lib():
         lib.xtg_set_options.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_uint64]
         lib.xtg_set_variance.argtypes = [C.c_void_p, C.c_double]
         lib.xtg_upload_counts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+        lib.xtg_nhicd_threshold_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p]
         _gpu = lib
     return _gpu
 
