@@ -38,6 +38,7 @@ import xtg  # noqa: E402
 
 WORKLOAD = dict(N=512, NT=64, NP=1024, n_ell=30, mu=0.01, I0=1e4, zfrac=0.005, seed=2)
 METRIC = "voxel-updates/s (ICD, plain 3D at scale: 512^2 x 64 voxels, 1024 views)"
+AMODES = {"fp32": xtg.XTG_A_FP32, "table32": xtg.XTG_A_TABLE32, "fp16": xtg.XTG_A_FP16}
 
 
 def params(w, radius=None):
@@ -142,7 +143,7 @@ def run_ours(args):
     w = WORKLOAD
     p, t, a, x_true, y, wt = make_data(w)
     ctx = xtg.Context(p, t, a)
-    ctx.set_options(a_mode=xtg.XTG_A_FP16 if args.afp16 else xtg.XTG_A_FP32, max_columns=args.columns)
+    ctx.set_options(a_mode=AMODES[args.amode], max_columns=args.columns)
     ctx.upload_sino(y, wt)
     ctx.init_error_sino()
     torch.cuda.synchronize()
@@ -214,7 +215,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded ellipsoid phantom, reference A, Poisson 1e4, 0.5% zingers)",
         "config": {"workload": "plain3d_512x512x64_1024views", "N_xy": 512, "N_z": 64, "N_r": 512, "N_t": 64,
-                   "N_p": 1024, "zinger": [4.0, 0.5], "nhicd": True, "a_mode": "fp16" if args.afp16 else "fp32",
+                   "N_p": 1024, "zinger": [4.0, 0.5], "nhicd": True, "a_mode": args.amode,
                    "iterations_timed": [args.warmup + 1, args.warmup + args.steps],
                    "l2": "inputs larger than L2 (e + w = 268 MB)", "parallelism": f"replicas{world}",
                    "cost_after": cost, "wall_s_timed": wall, "forward_projection_ms": fp_ms},
@@ -324,7 +325,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--afp16", action="store_true")
+    ap.add_argument("--amode", default="table32", choices=sorted(AMODES),
+                    help="A storage: table32 (exact FP32 column table), fp16 (FP16 column table), "
+                         "fp32 (computed at every column visit)")
     ap.add_argument("--columns", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

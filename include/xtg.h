@@ -44,11 +44,14 @@ enum {
 };
 
 /* A-matrix storage used by the ICD kernel.
- *   XTG_A_FP32: entries computed on the fly from H_r, bit-identical to
- *               calcAMatrixColumnforAngle (XT_AMatrix.c:50-110).
- *   XTG_A_FP16: entries precomputed once per context into HBM as FP16 with
- *               one FP32 scale per (frame, column). */
-enum { XTG_A_FP32 = 0, XTG_A_FP16 = 1 };
+ *   XTG_A_FP32:    entries computed in the kernel at every column visit,
+ *                  bit-identical to calcAMatrixColumnforAngle
+ *                  (XT_AMatrix.c:50-110); no extra memory.
+ *   XTG_A_TABLE32: the same FP32 entries precomputed once per context into
+ *                  an HBM column table (4 B offset + 4 B value per entry).
+ *   XTG_A_FP16:    the column table with FP16 values and one FP32 scale per
+ *                  (frame, column) -- the FP16-A precision form. */
+enum { XTG_A_FP32 = 0, XTG_A_FP16 = 1, XTG_A_TABLE32 = 2 };
 
 /* Update order.
  *   XTG_ORDER_PARALLEL: many columns in flight at once (the B200 schedule);
@@ -90,13 +93,6 @@ int xtg_get_hr(const xtg_ctx *ctx, float *hr /*[N_p][65]*/);
 /* Options: A storage, update order, concurrent columns (0 = device default),
  * seed of the GPU visiting order. */
 int xtg_set_options(xtg_ctx *ctx, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed);
-/* Forward projections (xtg_forward_project, xtg_init_error_sino, the FP64
- * resync and cost) either sum every sinogram entry over columns in the
- * reference's (row, column) order -- exact = 1, FP32 results bit-identical
- * to initErrorSinogam -- or accumulate in shared memory in any order --
- * exact = 0, the default, about an order of magnitude faster and equal to
- * the exact result up to FP32 rounding. */
-int xtg_set_exact_projection(xtg_ctx *ctx, int32_t exact);
 
 /* genSinogram_fromBin + computeWriteSinogram (XT_genSinogram.c:264-300,
  * XT_Engine.c:89-121): y, w and the offset d (NULL = zero).  Weights are
@@ -124,8 +120,9 @@ int xtg_set_variance(xtg_ctx *ctx, double var_est);
  * slots per triple, cnt the entry count. */
 int xtg_amatrix(xtg_ctx *ctx, int32_t n, const int32_t *rows, const int32_t *cols, const int32_t *views,
                 float *vals, int32_t *idx, int32_t *cnt);
-/* Forward projection A x of the current object, FP32, summed in the
- * reference's order (initErrorSinogam + forward_project_voxel_AMat1D,
+/* Forward projection A x of the current object, FP32, every sinogram entry
+ * summed over columns in the reference's (row, column) order, so the result
+ * is bit-identical to the reference's (initErrorSinogam + forward_project_voxel_AMat1D,
  * XT_ICD_update.c:551-569, XT_ForwardProject.c:8-25).  ax may be NULL
  * (result stays on the device). */
 int xtg_forward_project(xtg_ctx *ctx, float *ax);

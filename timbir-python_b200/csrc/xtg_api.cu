@@ -70,11 +70,16 @@ struct xtg_ctx {
   double *d_red = nullptr;       // [8][NSLOT] reduction slots
   double *d_absx = nullptr;      // [NSLOT]
   unsigned long long *d_cnt = nullptr;  // [4]
-  uint4 *d_a16 = nullptr;
-  float *d_a16s = nullptr;
-  int a16_vmax = 0, a16_ok = 0;
+  // A column table (CSC): entry runs per (frame, masked column)
+  long long *d_tstart = nullptr;
+  int *d_toff = nullptr;
+  float *d_tval32 = nullptr, *d_tscale = nullptr;
+  __half *d_tval16 = nullptr;
+  int table_mode = 0;  // 0 none, XTG_A_FP16 or XTG_A_TABLE32 when built
+  long long table_nnz = 0;
+  int table_max = 0;
   // options
-  int a_mode = XTG_A_FP32, order = XTG_ORDER_PARALLEL, max_columns = 0, exact_fp = 0;
+  int a_mode = XTG_A_FP32, order = XTG_ORDER_PARALLEL, max_columns = 0, span = 3;
   unsigned long long seed = 0x5eed5eedULL;
   int sm_count = 0;
   cudaStream_t st = nullptr;
@@ -142,209 +147,6 @@ __global__ void k_amatrix_batch(DevGeo G, const float *hr, const float *cosv, co
       k++;
     }
   cnt[i] = k;
-}
-
-struct FpArgs {
-  const float *x, *y, *d, *w, *hr, *cosv, *sinv;
-  const int *fov;
-  float *out;         // ax (MODE 0) or e (MODE 1, 2)
-  double *cost_slots; // MODE 2, 3
-  float T;
-  float delta;
-  double win_margin;
-};
-
-// MODE 0: out = A x (FP32); 1: out = e = y - A x - d (FP32);
-// 2: FP64 e64 = y - A x - d, out = (float)e64, data cost accumulated;
-// 3: FP64 data cost only.
-template <int MODE, int VF>
-__global__ void __launch_bounds__(256) k_fp(DevGeo G, FpArgs F) {
-  const int lane = threadIdx.x & 31;
-  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  double cacc = 0.0;
-  if (gw < (long long)G.N_p * G.N_r) {
-    const int p = (int)(gw / G.N_r), r = (int)(gw % G.N_r), fr = F.fov[p];
-    const float cp = F.cosv[p], sp = F.sinv[p];
-    const float *H = F.hr + (size_t)p * XT_HR_STRIDE;
-    // columns whose footprint can reach bin r: R0 + r dr - dxy <= r_col < R0 + (r+1) dr + dxy
-    const double lo = (double)G.R0 + (double)r * G.delta_r - G.delta_xy - F.win_margin;
-    const double hi = (double)G.R0 + (double)(r + 1) * G.delta_r + G.delta_xy + F.win_margin;
-    for (int tb = 0; tb < G.N_t; tb += 32 * VF) {
-      float accf[VF];
-      double accd[VF];
-#pragma unroll
-      for (int c = 0; c < VF; c++) {
-        accf[c] = 0.f;
-        accd[c] = 0.0;
-      }
-      for (int j = 0; j < G.N_y; j++) {
-        const float yv = xt_coord(G.y0, j, G.delta_xy);
-        const double ys = (double)yv * (double)sp;
-        int klo, khi;
-        if (fabs((double)cp) < 1e-12) {
-          if (-ys >= lo && -ys <= hi) {
-            klo = 0;
-            khi = G.N_x - 1;
-          } else {
-            continue;
-          }
-        } else {
-          double xa = (lo + ys) / (double)cp, xb = (hi + ys) / (double)cp;
-          if (xa > xb) {
-            const double t = xa;
-            xa = xb;
-            xb = t;
-          }
-          const double ka = (xa - (double)G.x0) / (double)G.delta_xy - 0.5;
-          const double kb = (xb - (double)G.x0) / (double)G.delta_xy - 0.5;
-          if (kb < -4.0 || ka > (double)G.N_x + 4.0) continue;
-          klo = max(0, (int)floor(ka) - 2);
-          khi = min(G.N_x - 1, (int)ceil(kb) + 2);
-        }
-        for (int kb0 = klo; kb0 <= khi; kb0 += 32) {
-          const int k = kb0 + lane;
-          const float a = (k <= khi) ? xt_amatrix_entry(G, H, cp, sp, j, k, r) : 0.f;
-          unsigned m = __ballot_sync(0xffffffffu, a != 0.f);
-          while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const float aa = __shfl_sync(0xffffffffu, a, l);
-            const float *xp = F.x + (((size_t)fr * G.N_y + j) * G.N_x + (kb0 + l)) * G.N_z;
-#pragma unroll
-            for (int c = 0; c < VF; c++) {
-              const int t = tb + lane * VF + c;
-              if (t < G.N_t) {
-                const float xv = __ldg(xp + t / G.zovl);
-                if (MODE <= 1)
-                  accf[c] = __fadd_rn(accf[c], __fmul_rn(xv, aa));
-                else
-                  accd[c] += (double)xv * (double)aa;
-              }
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < VF; c++) {
-        const int t = tb + lane * VF + c;
-        if (t >= G.N_t) continue;
-        const size_t o = ((size_t)p * G.N_r + r) * G.N_t + t;
-        if (MODE == 0) {
-          F.out[o] = accf[c];
-        } else if (MODE == 1) {
-          F.out[o] = __fsub_rn(__fsub_rn(F.y[o], accf[c]), F.d[(size_t)r * G.N_t + t]);
-        } else {
-          const double e64 = (double)F.y[o] - accd[c] - (double)F.d[(size_t)r * G.N_t + t];
-          if (MODE == 2) F.out[o] = (float)e64;
-          const double w64 = (double)F.w[o];
-          const double s = e64 * sqrt(w64);
-          if (fabs(s) < (double)F.T)
-            cacc += s * s;
-          else
-            cacc += 2.0 * (double)F.delta * (double)F.T * fabs(s) + (double)F.T * (double)F.T * (1.0 - 2.0 * (double)F.delta);
-        }
-      }
-    }
-  }
-  if (MODE >= 2) {
-    __shared__ double red[8];
-    for (int off = 16; off > 0; off >>= 1) cacc += __shfl_xor_sync(0xffffffffu, cacc, off);
-    if (lane == 0) red[threadIdx.x >> 5] = cacc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double s = 0;
-      for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += red[q];
-      atomicAdd(&F.cost_slots[blockIdx.x % NSLOT], s);
-    }
-  }
-}
-
-// Fast forward projection: one CTA per (view, block of detector rows) holds
-// that view's sinogram rows in shared memory.  Each warp takes 32 columns at
-// a time, every lane evaluates the exact A entries of one column, then the
-// warp walks those 32 columns with lanes over detector rows, loading each
-// column's z-line once and adding x*A into the shared accumulator
-// (shared-memory atomics; the summation order is not the reference's, so
-// results agree with the exact gather to FP32 rounding).  z-lines that are
-// all zero are skipped.
-// MODE 0: ax; 1: e = y - Ax - d (FP32); 2: e from FP64 sums + data cost; 3: cost only.
-template <int MODE, typename ACC, int NS>
-__global__ void __launch_bounds__(512) k_fp_fast(DevGeo G, FpArgs F, int tc) {
-  extern __shared__ __align__(16) unsigned char fp_smem[];
-  ACC *acc = reinterpret_cast<ACC *>(fp_smem);  // [N_r][tc]
-  const int p = blockIdx.x, t0 = blockIdx.y * tc;
-  const int nt = min(tc, G.N_t - t0);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int i = threadIdx.x; i < G.N_r * tc; i += blockDim.x) acc[i] = (ACC)0;
-  __syncthreads();
-  const int fr = F.fov[p];
-  const float cp = F.cosv[p], sp = F.sinv[p];
-  const float *H = F.hr + (size_t)p * XT_HR_STRIDE;
-  const int ncol = G.N_y * G.N_x;
-  for (int base = warp * 32; base < ncol; base += nwarp * 32) {
-    const int q = base + lane;
-    float vals[NS];
-    int first = 0, n = 0;
-    if (q < ncol) n = xt_amatrix_regs<NS>(G, H, cp, sp, q / G.N_x, q % G.N_x, vals, &first);
-    // columns in groups of 8: the 8 z-line loads are issued before any is
-    // used, so their L2 latencies overlap
-    for (int tb = 0; tb < nt; tb += 32) {
-      const int t = tb + lane;
-      for (int l0 = 0; l0 < 32; l0 += 8) {
-        float xv[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int ql = base + l0 + u;
-          xv[u] = (t < nt && ql < ncol) ? __ldg(F.x + ((size_t)fr * ncol + ql) * G.N_z + (t0 + t) / G.zovl) : 0.f;
-        }
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int l = l0 + u;
-          const int nl = __shfl_sync(0xffffffffu, n, l);
-          if (nl == 0 || __ballot_sync(0xffffffffu, xv[u] != 0.f) == 0) continue;
-          const int fl = __shfl_sync(0xffffffffu, first, l);
-#pragma unroll
-          for (int s = 0; s < NS; s++) {
-            if (s < nl) {
-              const float a = __shfl_sync(0xffffffffu, vals[s], l);
-              if (xv[u] != 0.f && a != 0.f) atomicAdd(&acc[(fl + s) * tc + t], (ACC)xv[u] * (ACC)a);
-            }
-          }
-        }
-      }
-    }
-  }
-  __syncthreads();
-  double cacc = 0.0;
-  for (int i = threadIdx.x; i < G.N_r * nt; i += blockDim.x) {
-    const int r = i / nt, t = i - r * nt;
-    const size_t o = ((size_t)p * G.N_r + r) * G.N_t + t0 + t;
-    const ACC s = acc[r * tc + t];
-    if (MODE == 0) {
-      F.out[o] = (float)s;
-    } else if (MODE == 1) {
-      F.out[o] = __fsub_rn(__fsub_rn(F.y[o], (float)s), F.d[(size_t)r * G.N_t + t0 + t]);
-    } else {
-      const double e64 = (double)F.y[o] - (double)s - (double)F.d[(size_t)r * G.N_t + t0 + t];
-      if (MODE == 2) F.out[o] = (float)e64;
-      const double sw = e64 * sqrt((double)F.w[o]);
-      if (fabs(sw) < (double)F.T)
-        cacc += sw * sw;
-      else
-        cacc += 2.0 * (double)F.delta * (double)F.T * fabs(sw) + (double)F.T * (double)F.T * (1.0 - 2.0 * (double)F.delta);
-    }
-  }
-  if (MODE >= 2) {
-    __shared__ double red[16];
-    for (int off = 16; off > 0; off >>= 1) cacc += __shfl_xor_sync(0xffffffffu, cacc, off);
-    if (lane == 0) red[warp] = cacc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double s = 0;
-      for (int w = 0; w < nwarp; w++) s += red[w];
-      atomicAdd(&F.cost_slots[(blockIdx.x + blockIdx.y * gridDim.x) % NSLOT], s);
-    }
-  }
 }
 
 // qGGMRF prior over forward neighbour pairs (XT_ICD_update.c:202-294), FP64.
@@ -664,48 +466,6 @@ __global__ void k_magsum(DevGeo G, int n_masked, const int *mcols, const float *
   }
 }
 
-// FP16 A records: per (frame, masked column, view) one uint4 =
-// {first | n << 16, half2(v0, v1), half2(v2, v3), 0}, values (A * delta_t)
-// divided by the column's largest value, which is kept in FP32.
-__global__ void k_build_a16(DevGeo G, const float *hr, const float *cosv, const float *sinv, const int *view_idx,
-                            const int *view_start, const int *view_num, int n_masked, const int *mcols, int vmax,
-                            uint4 *rec, float *scale) {
-  const int lane = threadIdx.x & 31;
-  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (gw >= (long long)G.N_time * n_masked) return;
-  const int f = (int)(gw / n_masked), ci = (int)(gw % n_masked);
-  const int c = mcols[ci], row = c / G.N_x, col = c % G.N_x;
-  const int V = view_num[f], vs = view_start[f];
-  float mx = 0.f;
-  for (int v = lane; v < V; v += 32) {
-    const int p = view_idx[vs + v];
-    float vals[XT_AMAX];
-    int first;
-    const int n = xt_amatrix_view(G, hr + (size_t)p * XT_HR_STRIDE, cosv[p], sinv[p], row, col, vals, &first);
-    for (int s = 0; s < n; s++) mx = fmaxf(mx, __fmul_rn(vals[s], G.delta_t));
-  }
-  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-  const float sc = mx > 0.f ? mx : 1.f;
-  if (lane == 0) scale[gw] = sc;
-  for (int v = lane; v < V; v += 32) {
-    const int p = view_idx[vs + v];
-    float vals[XT_AMAX];
-    int first;
-    int n = xt_amatrix_view(G, hr + (size_t)p * XT_HR_STRIDE, cosv[p], sinv[p], row, col, vals, &first);
-    n = min(n, 4);
-    float q[4];
-    for (int s = 0; s < 4; s++) q[s] = (s < n) ? __fmul_rn(vals[s], G.delta_t) / sc : 0.f;
-    const __half2 h01 = __floats2half2_rn(q[0], q[1]);
-    const __half2 h23 = __floats2half2_rn(q[2], q[3]);
-    uint4 r4;
-    r4.x = (unsigned)(first & 0xffff) | ((unsigned)n << 16);
-    r4.y = *reinterpret_cast<const unsigned *>(&h01);
-    r4.z = *reinterpret_cast<const unsigned *>(&h23);
-    r4.w = 0u;
-    rec[(size_t)gw * vmax + v] = r4;
-  }
-}
-
 // genSinogram_subsampleCounts (XT_genSinogram.c:303-374)
 __global__ void k_counts(DevGeo G, int mxy, int mz, const float *bright, const float *counts, float bh, float *y,
                          float *w) {
@@ -754,36 +514,7 @@ static cudaError_t launch_fp(xtg_ctx *c, float *out, double *slots) {
   F.fov = c->d_fov; F.out = out; F.cost_slots = slots; F.T = c->g.T; F.delta = c->g.delta;
   F.win_margin = 1e-4 * (double)c->g.N_r * c->g.delta_r + 1e-3 * c->g.delta_r;
   c->launches++;
-  if (c->exact_fp) {
-    // gather in the reference's summation order: FP32 results are bit-identical
-    const long long warps = (long long)c->g.N_p * c->g.N_r;
-    const unsigned grid = (unsigned)((warps + 7) / 8);
-    const int vf = std::min(4, std::max(1, (c->g.N_t + 31) / 32));
-    if (vf == 1)
-      k_fp<MODE, 1><<<grid, 256, 0, c->st>>>(c->G, F);
-    else if (vf == 2)
-      k_fp<MODE, 2><<<grid, 256, 0, c->st>>>(c->G, F);
-    else
-      k_fp<MODE, 4><<<grid, 256, 0, c->st>>>(c->G, F);
-    return cudaGetLastError();
-  }
-  const size_t esz = (MODE >= 2) ? sizeof(double) : sizeof(float);
-  const size_t budget = 200 * 1024;
-  int tc = (int)std::min<size_t>((size_t)c->g.N_t, budget / ((size_t)c->g.N_r * esz));
-  if (tc < 1) tc = 1;
-  const size_t smem = (size_t)c->g.N_r * tc * esz;
-  dim3 grid((unsigned)c->g.N_p, (unsigned)((c->g.N_t + tc - 1) / tc));
-  const int span = (int)ceil(2.0 * c->g.delta_xy / c->g.delta_r) + 1;
-  typedef void (*FpK)(DevGeo, FpArgs, int);
-  FpK k;
-  if (MODE >= 2)
-    k = span <= 3 ? k_fp_fast<MODE, double, 3> : span <= 4 ? k_fp_fast<MODE, double, 4> : k_fp_fast<MODE, double, 12>;
-  else
-    k = span <= 3 ? k_fp_fast<MODE, float, 3> : span <= 4 ? k_fp_fast<MODE, float, 4> : k_fp_fast<MODE, float, 12>;
-  cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  k<<<grid, 512, smem, c->st>>>(c->G, F, tc);
-  return cudaGetLastError();
+  return xtg::launch_fp(c->G, F, MODE, c->span, c->st);
 }
 
 extern "C" {
@@ -796,7 +527,8 @@ void xtg_destroy(xtg_ctx *c) {
   void *ptrs[] = {c->d_y, c->d_w, c->d_e, c->d_d, c->d_x, c->d_mag, c->d_hr, c->d_cos, c->d_sin, c->d_ax,
                   c->d_filt, c->d_tmp, c->d_num, c->d_den, c->d_thr, c->d_var, c->d_view_idx, c->d_view_start,
                   c->d_view_num, c->d_fov, c->d_mcols, c->d_rank, c->d_counter, c->d_nhcnt, c->d_err, c->d_kth,
-                  c->d_items, c->d_nh, c->d_red, c->d_absx, c->d_cnt, c->d_a16, c->d_a16s};
+                  c->d_items, c->d_nh, c->d_red, c->d_absx, c->d_cnt, c->d_tstart, c->d_toff, c->d_tval32,
+                  c->d_tscale, c->d_tval16};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -860,6 +592,7 @@ int xtg_create(const xt_params *prm, const double *times, const double *angles, 
       }
   c->n_masked = (int)c->mcols.size();
   for (int f = 0; f < g.N_time; f++) c->vmax = std::max(c->vmax, c->v.view_num[f]);
+  c->span = (int)ceil(2.0 * g.delta_xy / g.delta_r) + 1;  // detector bins a voxel can reach in one view
   rng_seed(c, 761521u);  // the reference seeds once in main (XT_Engine.c:137)
 
   int rc = 0;
@@ -944,25 +677,19 @@ int xtg_get_hr(const xtg_ctx *c, float *hr) {
 }
 
 int xtg_set_options(xtg_ctx *c, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed) {
-  if (!c || (a_mode != XTG_A_FP32 && a_mode != XTG_A_FP16) ||
+  if (!c || (a_mode != XTG_A_FP32 && a_mode != XTG_A_FP16 && a_mode != XTG_A_TABLE32) ||
       (order != XTG_ORDER_PARALLEL && order != XTG_ORDER_SEQUENTIAL) || max_columns < 0) {
     set_err("xtg_set_options: bad option");
     return XTG_E_ARG;
   }
-  if (a_mode == XTG_A_FP16 && (int)ceil(2.0 * c->g.delta_xy / c->g.delta_r) + 1 > 4) {
-    set_err("xtg_set_options: FP16 A supports delta_xy <= 1.5 detector bins");
-    return XTG_E_ARG;
+  if (a_mode != c->a_mode && c->table_mode != 0 && a_mode != XTG_A_FP32) {
+    // the entry offsets are shared; only the value array differs between table types
+    c->table_mode = 0;
   }
   c->a_mode = a_mode;
   c->order = order;
   c->max_columns = max_columns;
   c->seed = seed;
-  return 0;
-}
-
-int xtg_set_exact_projection(xtg_ctx *c, int32_t exact) {
-  if (!c) return XTG_E_ARG;
-  c->exact_fp = exact ? 1 : 0;
   return 0;
 }
 
@@ -1255,19 +982,51 @@ int xtg_update_variance(xtg_ctx *c) {
 }
 
 // ------------------------------------------------------------ ICD driver --
-static int ensure_a16(xtg_ctx *c) {
-  if (c->a16_ok) return 0;
-  c->a16_vmax = c->vmax;
-  const size_t nrec = (size_t)c->g.N_time * c->n_masked * c->a16_vmax;
-  if (!c->d_a16 && dalloc(c, &c->d_a16, nrec)) return XTG_E_CUDA;
-  if (!c->d_a16s && dalloc(c, &c->d_a16s, (size_t)c->g.N_time * c->n_masked)) return XTG_E_CUDA;
-  const long long warps = (long long)c->g.N_time * c->n_masked;
-  k_build_a16<<<(unsigned)((warps + 7) / 8), 256, 0, c->st>>>(c->G, c->d_hr, c->d_cos, c->d_sin, c->d_view_idx,
-                                                             c->d_view_start, c->d_view_num, c->n_masked, c->d_mcols,
-                                                             c->a16_vmax, c->d_a16, c->d_a16s);
-  c->launches++;
-  CK(cudaGetLastError());
-  c->a16_ok = 1;
+// Builds the A-matrix column table for the current a_mode (count pass, host
+// prefix sum, fill pass).  Rebuilt only when the value type changes.
+static int ensure_table(xtg_ctx *c) {
+  if (c->table_mode == c->a_mode) return 0;
+  const size_t ncol = (size_t)c->g.N_time * c->n_masked;
+  TableArgs T;
+  memset(&T, 0, sizeof(T));
+  T.hr = c->d_hr; T.cosv = c->d_cos; T.sinv = c->d_sin; T.view_idx = c->d_view_idx; T.view_start = c->d_view_start;
+  T.view_num = c->d_view_num; T.mcols = c->d_mcols; T.n_masked = c->n_masked;
+  if (!c->d_tstart && dalloc(c, &c->d_tstart, ncol + 1)) return XTG_E_CUDA;
+  CK(launch_table_count(c->G, T, c->span, c->d_tstart, c->st));
+  std::vector<long long> cnt(ncol + 1, 0);
+  CK(cudaMemcpyAsync(cnt.data(), c->d_tstart, ncol * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  long long run = 0, mx = 0;
+  for (size_t i = 0; i < ncol; i++) {
+    const long long n = cnt[i];
+    cnt[i] = run;
+    run += n;
+    mx = std::max(mx, n);
+  }
+  cnt[ncol] = run;
+  if (c->d_toff && c->table_nnz != run) {
+    set_err("A table size changed");
+    return XTG_E_STATE;
+  }
+  c->table_nnz = run;
+  c->table_max = (int)mx;
+  CK(cudaMemcpyAsync(c->d_tstart, cnt.data(), (ncol + 1) * 8, cudaMemcpyHostToDevice, c->st));
+  if (!c->d_toff && dalloc(c, &c->d_toff, (size_t)run)) return XTG_E_CUDA;
+  if (c->a_mode == XTG_A_FP16) {
+    if (!c->d_tval16 && dalloc(c, &c->d_tval16, (size_t)run)) return XTG_E_CUDA;
+    if (!c->d_tscale && dalloc(c, &c->d_tscale, ncol)) return XTG_E_CUDA;
+    T.val16 = c->d_tval16;
+    T.scale = c->d_tscale;
+  } else {
+    if (!c->d_tval32 && dalloc(c, &c->d_tval32, (size_t)run)) return XTG_E_CUDA;
+    T.val32 = c->d_tval32;
+  }
+  T.start = c->d_tstart;
+  T.off = c->d_toff;
+  CK(launch_table_fill(c->G, T, c->span, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->launches += 2;
+  c->table_mode = c->a_mode;
   return 0;
 }
 
@@ -1275,8 +1034,8 @@ static int ensure_a16(xtg_ctx *c) {
 static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, const int *n_dev, int use_perm,
                        unsigned long long key, int has_whole, int has_blocks, int seq_override) {
   const xt_geom &g = c->g;
-  if (c->a_mode == XTG_A_FP16) {
-    int rc = ensure_a16(c);
+  if (c->a_mode != XTG_A_FP32) {
+    int rc = ensure_table(c);
     if (rc) return rc;
   }
   const int seq = (seq_override >= 0) ? seq_override : (c->order == XTG_ORDER_SEQUENTIAL);
@@ -1294,32 +1053,34 @@ static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, c
     set_err("ICD work item of %d detector rows exceeds the kernel's %d (N_z/nzb too large)", rows, 32 * vec);
     return XTG_E_ARG;
   }
-  const int span = (int)ceil(2.0 * g.delta_xy / g.delta_r) + 1;
+  const int span = c->span;
   const int as = span <= 3 ? 3 : span <= 4 ? 4 : 12;
   if (span > 12) {
     set_err("delta_xy too large for the ICD kernel (%d bins per view)", span);
     return XTG_E_ARG;
   }
-  const int amode = (c->a_mode == XTG_A_FP16) ? 1 : 0;
+  const int amode = (c->a_mode == XTG_A_FP16) ? 1 : (c->a_mode == XTG_A_TABLE32) ? 2 : 0;
+  // shared memory per CTA: per-view slots (A in the kernel) or the longest column run (table)
+  const int vcap = amode ? c->table_max : c->vmax;
   IcdArgs A;
   memset(&A, 0, sizeof(A));
   A.e = c->d_e; A.w = c->d_w; A.x = c->d_x; A.magmap = c->d_mag; A.hr = c->d_hr; A.cosv = c->d_cos;
   A.sinv = c->d_sin; A.view_idx = c->d_view_idx; A.view_start = c->d_view_start; A.view_num = c->d_view_num;
   A.items = items; A.n_items_dev = n_dev; A.n_items = n; A.item_lo = lo; A.counter = c->d_counter;
-  A.use_perm = use_perm; A.perm_key = key; A.a16 = c->d_a16; A.a16_scale = c->d_a16s; A.col_rank = c->d_rank;
-  A.a16_vmax = c->a16_vmax; A.n_masked = c->n_masked; A.iter = iter;
+  A.use_perm = use_perm; A.perm_key = key; A.col_rank = c->d_rank; A.n_masked = c->n_masked; A.iter = iter;
+  A.tstart = c->d_tstart; A.toff = c->d_toff; A.tval32 = c->d_tval32; A.tval16 = c->d_tval16; A.tscale = c->d_tscale;
   A.T2 = g.T * g.T; A.Tdelta = g.T * g.delta; A.st_absx = c->d_absx; A.st_cnt = c->d_cnt; A.err = c->d_err;
   int grid;
   if (seq) {
     grid = 1;
   } else {
-    const int occ = icd_occupancy(vec, amode, 0, as, c->vmax, zmax, g.zovl);
+    const int occ = icd_occupancy(vec, amode, 0, as, vcap, zmax, g.zovl);
     grid = c->sm_count * occ;
     if (c->max_columns > 0) grid = std::min(grid, c->max_columns);
     if (!n_dev) grid = std::min(grid, std::max(n, 1));
   }
   CK(cudaMemsetAsync(c->d_counter, 0, 4, c->st));
-  CK(launch_icd(c->G, A, vec, amode, seq, as, c->vmax, zmax, grid, c->st));
+  CK(launch_icd(c->G, A, vec, amode, seq, as, vcap, zmax, grid, c->st));
   c->launches++;
   return 0;
 }
@@ -1674,8 +1435,8 @@ int xtg_update_columns(xtg_ctx *c, int32_t iter, int32_t n, const int32_t *items
       set_err("xtg_update_columns: item %d out of range", q);
       return XTG_E_ARG;
     }
-    if (c->a_mode == XTG_A_FP16 && c->col_rank[(size_t)r * g.N_x + k] < 0) {
-      set_err("xtg_update_columns: FP16 A covers masked columns only (item %d)", q);
+    if (c->a_mode != XTG_A_FP32 && c->col_rank[(size_t)r * g.N_x + k] < 0) {
+      set_err("xtg_update_columns: the A table covers masked columns only (item %d)", q);
       return XTG_E_ARG;
     }
     if (b >= 0) any_block = 1; else any_whole = 1;

@@ -61,10 +61,14 @@ __device__ __forceinline__ Nbr nbr_term(const DevGeo &G, const float *sNb, const
 template <int VEC, int AMODE, int SEQ, int AS>
 __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArgs A, int vmax, int zmax) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  int *sPack = reinterpret_cast<int *>(smem_raw);        // [vmax] first | n << 24
-  int *sView = sPack + vmax;                              // [vmax] view index p
+  // AMODE 0 (A computed here): per view {first | n << 24, view index, AS values}
+  int *sPack = reinterpret_cast<int *>(smem_raw);        // [vmax]
+  int *sView = sPack + vmax;                              // [vmax]
   float *sVal = reinterpret_cast<float *>(sView + vmax);  // [AS][vmax] A * delta_t
-  float *sRed = sVal + (size_t)vmax * AS;                 // [2][8][128] warp partials
+  // AMODE 1/2 (column table): the column's entry run, vmax = longest run
+  int *sOff = reinterpret_cast<int *>(smem_raw);         // [vmax] (p*N_r + bin)*N_t
+  float *sA = reinterpret_cast<float *>(sOff + vmax);    // [vmax] A * delta_t
+  float *sRed = (AMODE == 0) ? sVal + (size_t)vmax * AS : sA + vmax;  // [2][8][128] warp partials
   float *sTh = sRed + 2 * 8 * 128;                        // [2][zmax*zovl]
   const int rowsmax = zmax * G.zovl;
   float *sNb = sTh + 2 * rowsmax;                         // [9][zmax+2]
@@ -110,20 +114,16 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
 #pragma unroll
         for (int s = 0; s < AS; s++) sVal[s * vmax + v] = __fmul_rn(vals[s], G.delta_t);
       }
-    } else {
-      const int rk = A.col_rank[row * G.N_x + col];
-      const size_t rec = ((size_t)fr * A.n_masked + rk) * A.a16_vmax;
-      const float sc = A.a16_scale[(size_t)fr * A.n_masked + rk];
-      for (int v = tid; v < V; v += XTG_THREADS) {
-        const uint4 r4 = A.a16[rec + v];
-        const int first = (int)(r4.x & 0xffffu), n = (int)((r4.x >> 16) & 0xffu);
-        sPack[v] = first | (n << 24);
-        sView[v] = A.view_idx[vs + v];
-        const __half2 h01 = *reinterpret_cast<const __half2 *>(&r4.y);
-        const __half2 h23 = *reinterpret_cast<const __half2 *>(&r4.z);
-        const float hv[4] = {__low2float(h01), __high2float(h01), __low2float(h23), __high2float(h23)};
-#pragma unroll
-        for (int s = 0; s < AS; s++) sVal[s * vmax + v] = (s < 4) ? hv[s < 4 ? s : 0] * sc : 0.f;
+    }
+    int ne = 0;
+    if (AMODE != 0) {
+      const long long ti = (long long)fr * A.n_masked + A.col_rank[row * G.N_x + col];
+      const long long s0 = A.tstart[ti];
+      ne = (int)(A.tstart[ti + 1] - s0);
+      const float sc = (AMODE == 1) ? A.tscale[ti] : 1.f;
+      for (int e = tid; e < ne; e += XTG_THREADS) {
+        sOff[e] = __ldg(A.toff + s0 + e);
+        sA[e] = (AMODE == 2) ? __ldg(A.tval32 + s0 + e) : __half2float(A.tval16[s0 + e]) * sc;
       }
     }
     // 2. neighbourhood: the 3x3 columns' z-lines over [zb-1, ze+1], and the
@@ -153,55 +153,60 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     float th1[VEC], th2[VEC];
 #pragma unroll
     for (int c = 0; c < VEC; c++) th1[c] = th2[c] = 0.f;
+    // one footprint entry: rows [base, base + VEC) of one (view, bin), weight a
+    auto accumulate = [&](size_t base, float a) {
+      const float a2 = a * a;
+      float ev[VEC], wv[VEC];
+      if (VEC == 4) {
+        const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(A.e + base));
+        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(A.w + base));
+        ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
+        wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
+      } else {
+#pragma unroll
+        for (int c = 0; c < VEC; c++) {
+          ev[c] = __ldcg(A.e + base + c);
+          wv[c] = __ldg(A.w + base + c);
+        }
+      }
+      // generalized-Huber (zinger) weight: w where |e sqrt(w)| < T, else
+      // T delta sqrt(w) / |e| (XT_VoxUpdate.c:34-48); the slow branch runs
+      // only when some lane of the warp needs it
+      float ew[VEC];
+      bool zg = false;
+#pragma unroll
+      for (int c = 0; c < VEC; c++) {
+        ew[c] = ev[c] * wv[c];
+        zg |= (ev[c] * ew[c] >= A.T2);
+      }
+      if (__any_sync(__activemask(), zg)) {
+#pragma unroll
+        for (int c = 0; c < VEC; c++) {
+          float we = wv[c];
+          if (ev[c] * ew[c] >= A.T2) we = __fdividef(A.Tdelta * sqrtf(wv[c]), fabsf(ev[c]));
+          th2[c] = fmaf(a2, we, th2[c]);
+          th1[c] = fmaf(-a * ev[c], we, th1[c]);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < VEC; c++) {
+          th2[c] = fmaf(a2, wv[c], th2[c]);
+          th1[c] = fmaf(-a, ew[c], th1[c]);
+        }
+      }
+    };
     if (tl < tln) {
       const int trow = t0 + tl * VEC;
-      for (int v = vg; v < V; v += vgs) {
-        const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
-        const size_t base = ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
+      if (AMODE == 0) {
+        for (int v = vg; v < V; v += vgs) {
+          const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
+          const size_t base = ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
 #pragma unroll
-        for (int s = 0; s < AS; s++) {
-          if (s < n) {
-            const float a = sVal[s * vmax + v], a2 = a * a;
-            float ev[VEC], wv[VEC];
-            if (VEC == 4) {
-              const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(A.e + base + (size_t)s * G.N_t));
-              const float4 w4 = __ldg(reinterpret_cast<const float4 *>(A.w + base + (size_t)s * G.N_t));
-              ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
-              wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
-            } else {
-#pragma unroll
-              for (int c = 0; c < VEC; c++) {
-                ev[c] = __ldcg(A.e + base + (size_t)s * G.N_t + c);
-                wv[c] = __ldg(A.w + base + (size_t)s * G.N_t + c);
-              }
-            }
-            // generalized-Huber (zinger) weight: w where |e sqrt(w)| < T,
-            // else T delta sqrt(w) / |e| (XT_VoxUpdate.c:34-48); the slow
-            // branch runs only when some lane of the warp needs it
-            float ew[VEC];
-            bool zg = false;
-#pragma unroll
-            for (int c = 0; c < VEC; c++) {
-              ew[c] = ev[c] * wv[c];
-              zg |= (ev[c] * ew[c] >= A.T2);
-            }
-            if (__any_sync(__activemask(), zg)) {
-#pragma unroll
-              for (int c = 0; c < VEC; c++) {
-                float we = wv[c];
-                if (ev[c] * ew[c] >= A.T2) we = __fdividef(A.Tdelta * sqrtf(wv[c]), fabsf(ev[c]));
-                th2[c] = fmaf(a2, we, th2[c]);
-                th1[c] = fmaf(-a * ev[c], we, th1[c]);
-              }
-            } else {
-#pragma unroll
-              for (int c = 0; c < VEC; c++) {
-                th2[c] = fmaf(a2, wv[c], th2[c]);
-                th1[c] = fmaf(-a, ew[c], th1[c]);
-              }
-            }
-          }
+          for (int s = 0; s < AS; s++)
+            if (s < n) accumulate(base + (size_t)s * G.N_t, sVal[s * vmax + v]);
         }
+      } else {
+        for (int e = vg; e < ne; e += vgs) accumulate((size_t)sOff[e] + trow, sA[e]);
       }
     }
     // reduce over view groups: lanes with equal tl inside a warp, then warps
@@ -383,22 +388,25 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
       }
       if (any) {
         const int trow = t0 + tl * VEC;
-        for (int v = vg; v < V; v += vgs) {
-          const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
-          float *ep = A.e + ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
+        auto scatter = [&](float *ep, float a) {
+          if (VEC == 4) {
+            xt_red_add4(ep, -(a * dv[0]), -(a * dv[1]), -(a * dv[2]), -(a * dv[3]));
+          } else {
 #pragma unroll
-          for (int s = 0; s < AS; s++) {
-            if (s < n) {
-              const float a = sVal[s * vmax + v];
-              if (VEC == 4) {
-                xt_red_add4(ep + (size_t)s * G.N_t, -(a * dv[0]), -(a * dv[1]), -(a * dv[2]), -(a * dv[3]));
-              } else {
-#pragma unroll
-                for (int c = 0; c < VEC; c++)
-                  if (dv[c] != 0.f) atomicAdd(ep + (size_t)s * G.N_t + c, -(a * dv[c]));
-              }
-            }
+            for (int c = 0; c < VEC; c++)
+              if (dv[c] != 0.f) atomicAdd(ep + c, -(a * dv[c]));
           }
+        };
+        if (AMODE == 0) {
+          for (int v = vg; v < V; v += vgs) {
+            const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
+            float *ep = A.e + ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
+#pragma unroll
+            for (int s = 0; s < AS; s++)
+              if (s < n) scatter(ep + (size_t)s * G.N_t, sVal[s * vmax + v]);
+          }
+        } else {
+          for (int e = vg; e < ne; e += vgs) scatter(A.e + (size_t)sOff[e] + trow, sA[e]);
         }
       }
     }
@@ -406,36 +414,43 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
   }
 }
 
-size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as) {
+size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode) {
   size_t b = 0;
-  b += (size_t)vmax * 4 * 2;         // sPack, sView
-  b += (size_t)vmax * as * 4;        // sVal
-  b += 2 * 8 * 128 * 4;              // sRed
-  b += 2 * (size_t)zmax * zovl * 4;  // sTh
-  b += 9 * (size_t)(zmax + 2) * 4;   // sNb
-  b += 2 * (size_t)zmax * 4;         // sTn
-  b += (size_t)zmax * 4;             // sDelta
+  if (amode == 0)
+    b += (size_t)vmax * (4 * 2 + 4 * (size_t)as);  // sPack, sView, sVal
+  else
+    b += (size_t)vmax * 8;                         // sOff, sA (vmax = longest column run)
+  b += 2 * 8 * 128 * 4;                            // sRed
+  b += 2 * (size_t)zmax * zovl * 4;                // sTh
+  b += 9 * (size_t)(zmax + 2) * 4;                 // sNb
+  b += 2 * (size_t)zmax * 4;                       // sTn
+  b += (size_t)zmax * 4;                           // sDelta
   return b;
 }
 
 typedef void (*IcdKernel)(DevGeo, IcdArgs, int, int);
 
-// slot count: 3 covers delta_xy <= delta_r, 4 covers delta_xy <= 1.5 delta_r,
-// 12 covers delta_xy <= 5.5 delta_r
+// A computed in the kernel (amode 0): slot count 3 covers delta_xy <= delta_r,
+// 4 covers delta_xy <= 1.5 delta_r, 12 covers delta_xy <= 5.5 delta_r.  The
+// table modes (1 = FP16, 2 = FP32) have no per-view slots.
 static IcdKernel icd_kernel(int vec, int amode, int seq, int as) {
-#define XTG_K(V, M, S) (as == 3 ? k_icd_columns<V, M, S, 3> : as == 4 ? k_icd_columns<V, M, S, 4> : k_icd_columns<V, M, S, 12>)
+#define XTG_K(V, S) (as == 3 ? k_icd_columns<V, 0, S, 3> : as == 4 ? k_icd_columns<V, 0, S, 4> : k_icd_columns<V, 0, S, 12>)
+#define XTG_T(V, M, S) k_icd_columns<V, M, S, 3>
   if (vec == 4) {
-    if (amode == 0) return seq ? XTG_K(4, 0, 1) : XTG_K(4, 0, 0);
-    return seq ? XTG_K(4, 1, 1) : XTG_K(4, 1, 0);
+    if (amode == 0) return seq ? XTG_K(4, 1) : XTG_K(4, 0);
+    if (amode == 1) return seq ? XTG_T(4, 1, 1) : XTG_T(4, 1, 0);
+    return seq ? XTG_T(4, 2, 1) : XTG_T(4, 2, 0);
   }
-  if (amode == 0) return seq ? XTG_K(1, 0, 1) : XTG_K(1, 0, 0);
-  return seq ? XTG_K(1, 1, 1) : XTG_K(1, 1, 0);
+  if (amode == 0) return seq ? XTG_K(1, 1) : XTG_K(1, 0);
+  if (amode == 1) return seq ? XTG_T(1, 1, 1) : XTG_T(1, 1, 0);
+  return seq ? XTG_T(1, 2, 1) : XTG_T(1, 2, 0);
 #undef XTG_K
+#undef XTG_T
 }
 
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st) {
-  const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as);
+  const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as, amode);
   IcdKernel k = icd_kernel(vec, amode, seq, as);
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -449,7 +464,7 @@ cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, in
 }
 
 int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl) {
-  const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as);
+  const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as, amode);
   IcdKernel k = icd_kernel(vec, amode, seq, as);
   int nb = 0;
   cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

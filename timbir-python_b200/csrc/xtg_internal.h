@@ -18,10 +18,15 @@ struct IcdArgs {
   int *counter;
   int use_perm;
   unsigned long long perm_key;
-  const uint4 *a16;        // FP16 A records [frame][col_rank][vmax] or null
-  const float *a16_scale;  // [frame][col_rank]
-  const int *col_rank;     // [N_y*N_x] -> rank in the masked list, -1 outside
-  int a16_vmax, n_masked;
+  // A column table (a_mode FP16 / FP32 table): entries of (frame, masked
+  // column rank) at [tstart[i], tstart[i+1]), i = frame * n_masked + rank
+  const long long *tstart;
+  const int *toff;          // (p * N_r + bin) * N_t of each entry
+  const float *tval32;      // A * delta_t (FP32 table)
+  const __half *tval16;     // A * delta_t / scale (FP16 table)
+  const float *tscale;      // per (frame, column) scale of the FP16 table
+  const int *col_rank;      // [N_y*N_x] -> rank in the masked list, -1 outside
+  int n_masked;
   int iter;
   float T2, Tdelta;
   double *st_absx;             // [64] slots
@@ -29,7 +34,34 @@ struct IcdArgs {
   int *err;
 };
 
-size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as);
+#define FP_WARPS 4  // warps per projector CTA, 32 detector bins each
+
+struct FpArgs {
+  const float *x, *y, *d, *w, *hr, *cosv, *sinv;
+  const int *fov;
+  float *out;          // ax (mode 0) or e (modes 1, 2)
+  double *cost_slots;  // modes 2, 3: 64 slots
+  float T;
+  float delta;
+  double win_margin;
+};
+
+struct TableArgs {
+  const float *hr, *cosv, *sinv;
+  const int *view_idx, *view_start, *view_num, *mcols;
+  int n_masked;
+  const long long *start;
+  int *off;
+  float *val32;
+  __half *val16;
+  float *scale;
+};
+
+cudaError_t launch_fp(const DevGeo &G, const FpArgs &F, int mode, int ns, cudaStream_t st);
+cudaError_t launch_table_count(const DevGeo &G, const TableArgs &T, int ns, long long *count, cudaStream_t st);
+cudaError_t launch_table_fill(const DevGeo &G, const TableArgs &T, int ns, cudaStream_t st);
+
+size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode);
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st);
 int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl);

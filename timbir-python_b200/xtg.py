@@ -20,14 +20,14 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(HERE, "lib")
 
-XTG_A_FP32, XTG_A_FP16 = 0, 1
+XTG_A_FP32, XTG_A_FP16, XTG_A_TABLE32 = 0, 1, 2
 XTG_ORDER_PARALLEL, XTG_ORDER_SEQUENTIAL = 0, 1
 
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
     "xtg_create", "xtg_destroy", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
     "xtg_get_hr", "xtg_set_options", "xtg_upload_sino", "xtg_upload_counts", "xtg_upload_object",
-    "xtg_set_exact_projection", "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
+    "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
     "xtg_get_offset", "xtg_set_offset", "xtg_get_magmap", "xtg_set_magmap", "xtg_get_variance",
     "xtg_set_variance", "xtg_amatrix", "xtg_forward_project", "xtg_init_error_sino",
     "xtg_resync_fp64", "xtg_map_cost_fp64", "xtg_map_cost_running", "xtg_zinger_refresh",
@@ -286,9 +286,6 @@ class Context:
 
     def set_options(self, a_mode=XTG_A_FP32, order=XTG_ORDER_PARALLEL, max_columns=0, seed=0x5EED5EED):
         _check(self.lib.xtg_set_options(self.h, a_mode, order, max_columns, seed), "xtg_set_options")
-
-    def set_exact_projection(self, exact=True):
-        _check(self.lib.xtg_set_exact_projection(self.h, 1 if exact else 0), "xtg_set_exact_projection")
 
     def upload_sino(self, y, w, d=None):
         y, w = _f32(y), _f32(w)
