@@ -18,7 +18,7 @@ runs and the object comes back device->host.
 --impl reference times the reference engine's own CPU implementation
 (oracle/_ref, compiled from the reference sources, OpenMP on every host core)
 on a bounded sample of the same workload: the same geometry, views and data
-restricted by --radius_obj to a central disk of 1/16 of the columns.
+restricted by --radius_obj to a central disk (radius N/8, about 1/20 of the columns).
 """
 import argparse
 import json
@@ -36,25 +36,60 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "timbir-python_b200")]
 
 import xtg  # noqa: E402
 
-WORKLOAD = dict(N=512, NT=64, NP=1024, n_ell=30, mu=0.01, I0=1e4, zfrac=0.005, seed=2)
-METRIC = "voxel-updates/s (ICD, plain 3D at scale: 512^2 x 64 voxels, 1024 views)"
+WORKLOADS = {
+    # plain 3D at scale: 64 slices of 512^2, 512 bins x 64 rows, 1024 views
+    # uniform over 180 deg, 30 ellipsoids, 1e4 photons/ray, 0.5 % zingers,
+    # zinger correction on (T = 4, delta = 0.5), NHICD on
+    "plain3d": dict(N=512, NT=64, NP=1024, n_time=1, n_ell=30, mu=0.01, I0=1e4, zfrac=0.005, seed=2,
+                    zinger=True, interlaced=None, moving=0),
+    # 4D TIMBIR: 256^2 x 16 volume x 16 time frames, 8 interlaced sub-frames of
+    # 32 views per rotation in bit-reversed order (N_theta = 256), 2 sub-frames
+    # (64 views) per frame, 1024 views, 256 bins x 16 rows; 8 ellipsoids moving
+    # up to 1 voxel/frame plus one growing; temporal prior weight 0.5
+    "timbir4d": dict(N=256, NT=16, NP=1024, n_time=16, n_ell=8, mu=0.01, I0=1e4, zfrac=0.0, seed=3,
+                     zinger=False, interlaced=(8, 256), moving=8),
+}
+WORKLOAD = WORKLOADS["plain3d"]
+METRIC = "voxel-updates/s (ICD)"
+# DRAM bytes per voxel update of the ICD column kernel, from the committed ncu
+# summary of a random-pass (chunk) launch; scaled by voxel updates per launch
+PROFILE = os.path.join(ROOT, "profiles", "icd_columns_plain3d.md")
 AMODES = {"fp32": xtg.XTG_A_FP32, "table32": xtg.XTG_A_TABLE32, "fp16": xtg.XTG_A_FP16}
+# bytes per A entry streamed from HBM: computed in registers, FP32 table, FP16 table
+A_BYTES = {"fp32": 0.0, "table32": 8.0, "fp16": 6.0}
+# the reference's HU conversion of --sigma_s / --sigma_t (XT_Init.c:510-511)
+SLOPE_HU = 1000.0 / (0.521225397034623 - 0.496372335005353 * 0.001205) / 0.0001
+C_HU = -SLOPE_HU * (0.496372335005353 * 0.001205 * 0.0001)
+
+
+def sigma_t_arg(sigma_s_arg, delta_rtime, weight):
+    """--sigma_t giving the temporal prior `weight` times the spatial one:
+    (sigma_t delta_Rtime)^2 = (sigma_s mult_xy)^2 / weight (q = 2, mult_xy = 1)."""
+    s = (sigma_s_arg - C_HU) / SLOPE_HU
+    return C_HU + SLOPE_HU * s / (delta_rtime * weight ** 0.5)
 
 
 def params(w, radius=None):
-    N = w["N"]
+    N, nt = w["N"], w["n_time"]
+    rdelta = float(w["NP"] // nt)
+    sig = 200000.0
     return xtg.Params(
-        p=1.2, sigma_s=200000.0, sigma_t=200000.0, c_s=0.01, c_t=0.01, delta_xy=1.0, delta_z=1.0,
-        length_r=float(N), length_t=float(w["NT"]), rotation_center=N / 2.0, alpha=1.0, Rtime0=0.0,
-        Rtime_delta=float(w["NP"]), radius_obj=float(N) if radius is None else float(radius),
-        zingerT=4.0, zingerDel=0.5, iter=100, Rtime_num=1, num_projections=w["NP"], N_r=N, N_t=w["NT"],
-        num_threads=1, positivity=1, no_NHICD=0)
+        p=1.2, sigma_s=sig, sigma_t=sigma_t_arg(sig, rdelta, 0.5) if nt > 1 else sig, c_s=0.01, c_t=0.01,
+        delta_xy=1.0, delta_z=1.0, length_r=float(N), length_t=float(w["NT"]), rotation_center=N / 2.0, alpha=1.0,
+        Rtime0=0.0, Rtime_delta=rdelta, radius_obj=float(N) if radius is None else float(radius),
+        zingerT=4.0 if w["zinger"] else 100000.0, zingerDel=0.5 if w["zinger"] else 0.0, iter=100, Rtime_num=nt,
+        num_projections=w["NP"], N_r=N, N_t=w["NT"], num_threads=1, positivity=1, no_NHICD=0)
 
 
 def make_data(w):
     p = params(w)
-    t, a = xtg.round_views(*xtg.views_uniform(w["NP"]))
-    x = xtg.phantom((1, w["NT"], w["N"], w["N"]), w["n_ell"], w["mu"], w["seed"])
+    if w["interlaced"]:
+        t, a = xtg.round_views(*xtg.views_interlaced(*w["interlaced"], w["NP"]))
+    else:
+        t, a = xtg.round_views(*xtg.views_uniform(w["NP"]))
+    mv = w["moving"]
+    x = xtg.phantom((w["n_time"], w["NT"], w["N"], w["N"]), w["n_ell"], w["mu"], w["seed"], n_moving=mv,
+                    max_shift=1.0 if mv else 0.0, growing=1 if mv else 0)
     ax = xtg.forward_cpu(p, t, a, x)
     y, wt = xtg.measure(ax, w["I0"], w["seed"] + 100, zinger_frac=w["zfrac"])
     return p, t, a, x, y, wt
@@ -99,15 +134,83 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch():
-    """DRAM bytes per ICD launch from the committed ncu summary, if present."""
-    f = os.path.join(ROOT, "profiles", "icd_columns_plain3d_512.md")
-    if not os.path.exists(f):
+def dram_bytes_per_update():
+    """DRAM bytes per voxel update of the ICD kernel from the committed ncu summary."""
+    if not os.path.exists(PROFILE):
         return None
-    for line in open(f):
-        if line.startswith("traffic_bytes_per_chunk_launch:"):
+    for line in open(PROFILE):
+        if line.startswith("dram_bytes_per_voxel_update:"):
             return float(line.split(":")[1])
     return None
+
+
+def workload_name(w):
+    if w["n_time"] > 1:
+        return f"timbir4d_{w['N']}x{w['N']}x{w['NT']}x{w['n_time']}frames_{w['NP']}views"
+    return f"plain3d_{w['N']}x{w['N']}x{w['NT']}_{w['NP']}views"
+
+
+def workload(args):
+    w = dict(WORKLOADS[args.workload])
+    if args.nxy:
+        w["N"] = args.nxy
+    return w
+
+
+def base_config(w, amode):
+    return {"workload": workload_name(w), "N_xy": w["N"], "N_z": w["NT"], "N_time": w["n_time"], "N_r": w["N"],
+            "N_t": w["NT"], "N_p": w["NP"], "views": "interlaced K=%d N_theta=%d" % w["interlaced"]
+            if w["interlaced"] else "uniform", "zinger": [4.0, 0.5] if w["zinger"] else None,
+            "zinger_frac": w["zfrac"], "temporal_weight": 0.5 if w["n_time"] > 1 else None, "nhicd": True,
+            "a_mode": amode}
+
+
+def converge(ctx, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10):
+    """Seconds to MAP cost <= (1 + tol) C*.
+
+    Pass 1 (untimed) reconstructs from x = 0 until the FP64 MAP cost stalls
+    (relative decrease over 10 iterations below `stall`, or `max_iters`); its
+    final FP64 cost (full resync e = y - Ax - d) is C*.  Pass 2 starts again
+    from x = 0 and is timed on the wall clock, cost test included: after every
+    iteration the MAP cost of the running error sinogram (FP64 sums), every
+    `resync_every` iterations and at the stop the FP64 resync; it stops at the
+    first FP64-resynced cost <= (1 + tol) C*."""
+    import torch
+    zero = np.zeros(ctx.obj_shape, np.float32)
+
+    def restart():
+        ctx.upload_object(zero)
+        ctx.init_error_sino()
+        torch.cuda.synchronize()
+
+    restart()
+    hist = []
+    for it in range(1, max_iters + 1):
+        ctx.iteration(it)
+        c = ctx.resync_fp64()[0] if it % resync_every == 0 else ctx.cost_running()[0]
+        hist.append(c)
+        if it >= 20 and (hist[-11] - hist[-1]) < stall * abs(hist[-1]):
+            break
+    c_star = ctx.resync_fp64()[0]
+    iters_star = len(hist)
+    target = c_star * (1.0 + tol)
+    restart()
+    t0 = time.perf_counter()
+    it, c = 0, float("inf")
+    while it < max_iters:
+        it += 1
+        ctx.iteration(it)
+        c = ctx.cost_running()[0]
+        if c <= target or it % resync_every == 0:
+            c = ctx.resync_fp64()[0]
+            if c <= target:
+                break
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    return {"s": secs if c <= target else None, "iterations": it, "cost": c, "c_star": c_star,
+            "c_star_iterations": iters_star, "tol": tol,
+            "c_star_source": "this engine run to a stall (FP64 resync cost); the FP64 CPU oracle's converged "
+                             "cost is the reference at test sizes"}
 
 
 def nnz_per_column(ctx, n_cols=512, seed=0):
@@ -125,6 +228,20 @@ def nnz_per_column(ctx, n_cols=512, seed=0):
     return float(cnt.sum()) / len(keep)
 
 
+def job_totals(ms, updates, world, device):
+    """Whole-job figures of N independent replicas: the slowest rank's device
+    time (max over ranks) and the voxel updates of all ranks (sum)."""
+    if world <= 1:
+        return float(ms), float(updates)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms), float(updates)], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(t[1])
+
+
 def dist_setup():
     n = int(os.environ.get("WORLD_SIZE", "1"))
     r = int(os.environ.get("RANK", "0"))
@@ -140,10 +257,11 @@ def run_ours(args):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    w = WORKLOAD
+    w = workload(args)
     p, t, a, x_true, y, wt = make_data(w)
     ctx = xtg.Context(p, t, a)
     ctx.set_options(a_mode=AMODES[args.amode], max_columns=args.columns)
+    ctx.set_zslab(args.zslab)
     ctx.upload_sino(y, wt)
     ctx.init_error_sino()
     torch.cuda.synchronize()
@@ -160,29 +278,24 @@ def run_ours(args):
     torch.cuda.synchronize()
     launches0 = ctx.launch_count()
     clk = Clocks(lrank)
-    ms_tot, upd, kms, rows = 0.0, 0, 0.0, 0
+    ms_tot, upd, kms, rows, n_icd, zsk = 0.0, 0, 0.0, 0, 0, 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
         it += 1
         st = ctx.iteration(it)
         ms_tot += st.ms
         upd += st.voxel_updates
-        k_ms, _ = ctx.last_kernel_time()
+        zsk += st.zero_skipped
+        k_ms, _, k_n = ctx.last_kernel_time()
         kms += k_ms
+        n_icd += k_n
         rows += st.columns
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     clocks = clk.stop()
     launches = ctx.launch_count() - launches0
     cost = ctx.cost()[0]
-    if world > 1:
-        tt = torch.tensor([ms_tot, float(upd)], dtype=torch.float64, device="cuda")
-        mx = tt.clone()
-        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.SUM)
-        ms_job, upd_job = float(mx[0]), float(tt[1])
-    else:
-        ms_job, upd_job = ms_tot, float(upd)
+    ms_job, upd_job = job_totals(ms_tot, upd, world, "cuda")
     value = upd_job / (ms_job / 1e3)
 
     # e2e: through the C ABI from pinned host buffers, host<->device inside the region
@@ -202,33 +315,44 @@ def run_ours(args):
         e2e_upd += st.voxel_updates
     e2e = e2e_upd / e2e_t * world
 
-    # roofline of the ICD column kernel: algorithmic bytes = rows x nnz x 12 B
-    # (e read, w read, e write per (view, bin, row)), per ICD launch time
-    n_items = rows
-    rows_touched = upd * p.delta_z  # every updated voxel streams its zovl rows
-    alg_bytes = rows_touched * nnz * 12.0
+    # roofline of the ICD column kernel.  Algorithmic bytes per voxel update:
+    # nnz x zovl x 12 B (e read, w read, e write per (view, bin, row)) plus the
+    # column's A entries shared by its N_z voxels; per average ICD launch
+    b_upd = nnz * ctx.zovl * 12.0 + nnz * A_BYTES[args.amode] / ctx.N_z
+    alg_per_launch = upd * b_upd / max(n_icd, 1)
+    ms_per_launch = kms / max(n_icd, 1)
     peak, kind = peaks()
-    achieved = alg_bytes / (kms / 1e3) / 1e9 if kms > 0 else 0.0
+    achieved = alg_per_launch / (ms_per_launch / 1e3) / 1e9 if kms > 0 else 0.0
+    dpu = dram_bytes_per_update()
+    traffic = dpu * upd / max(n_icd, 1) if dpu else None
     line = {
         "metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_job / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded ellipsoid phantom, reference A, Poisson 1e4, 0.5% zingers)",
-        "config": {"workload": "plain3d_512x512x64_1024views", "N_xy": 512, "N_z": 64, "N_r": 512, "N_t": 64,
-                   "N_p": 1024, "zinger": [4.0, 0.5], "nhicd": True, "a_mode": args.amode,
+        "data": f"synthetic (seeded ellipsoid phantom{', moving' if w['moving'] else ''}, reference A, "
+                f"Poisson {w['I0']:.0e} photons/ray, {100 * w['zfrac']:g}% zingers)",
+        "config": {**base_config(w, args.amode), "masked_columns": ctx.n_masked, "zslab": ctx.zslab(),
                    "iterations_timed": [args.warmup + 1, args.warmup + args.steps],
-                   "l2": "inputs larger than L2 (e + w = 268 MB)", "parallelism": f"replicas{world}",
-                   "cost_after": cost, "wall_s_timed": wall, "forward_projection_ms": fp_ms},
+                   "l2": f"inputs larger than L2 (e + w = {2 * y.nbytes / 1e6:.0f} MB)",
+                   "parallelism": f"replicas{world}",
+                   "cost_after": cost, "wall_s_timed": wall, "forward_projection_ms": fp_ms,
+                   "zero_skipped_per_step": zsk / args.steps,
+                   "counted": "voxel updates exclude zero-skipped voxels (x = 0 with no positive neighbour)"},
         "e2e": {"value": e2e, "unit": "voxel-updates/s", "h2d_bytes_per_step": int(y.nbytes + wt.nbytes),
                 "d2h_bytes_per_step": int(xo.numel() * 4)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic_per_launch(),
-                     "peak_kind": peak_kind_note(kind),
-                     "bytes_per_voxel_update": nnz * 12.0, "nnz_per_column": nnz,
-                     "kernel_ms_per_step": kms / args.steps, "column_items_per_step": n_items / args.steps},
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind_note(kind), "kernel": "k_icd_columns",
+                     "alg_bytes_per_launch": alg_per_launch, "ms_per_launch": ms_per_launch,
+                     "icd_launches_timed": n_icd, "bytes_per_voxel_update": b_upd, "nnz_per_column": nnz,
+                     "dram_bytes_per_voxel_update": dpu,
+                     "traffic_note": "ncu dram bytes per voxel update of a random-pass launch x voxel updates per launch",
+                     "kernel_ms_per_step": kms / args.steps, "column_items_per_step": rows / args.steps},
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if not args.no_converge:
+        line["time_to_cost"] = converge(ctx)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
@@ -242,16 +366,15 @@ def peak_kind_note(kind):
     return f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "fallback 6.65 TB/s"
 
 
-def ref_sample_run(iters=1, threads=None):
+def ref_sample_run(w, iters=1, threads=None):
     """Times the reference engine's own updateVoxelsTimeSlices (oracle/_ref,
     via oracle/ref_harness.c) on the bounded sample; returns
     (voxel updates/s, seconds, voxels per iteration, threads)."""
     from oracle.oracle import Reference, ref_available
     if not ref_available():
         return None
-    w = WORKLOAD
     threads = threads or os.cpu_count()
-    radius = w["N"] / 8.0  # central disk: about 1/16 of the columns
+    radius = w["N"] / 8.0  # central disk: about 1/20 of the columns
     p, t, a, x_true, y, wt = make_data(w)
     p.radius_obj = radius
     p.num_threads = threads
@@ -270,7 +393,7 @@ def ref_sample_run(iters=1, threads=None):
         c = np.arange(w["N"]) + 0.5 - w["N"] / 2.0
         n_masked = int(((c[None, :] ** 2 + c[:, None] ** 2) < radius * radius).sum())
         g = None
-        vox = n_masked * w["NT"]
+        vox = n_masked * w["NT"] * w["n_time"]
         t0 = time.perf_counter()
         for it in range(1, iters + 1):
             r.iterate(it)
@@ -282,14 +405,14 @@ def ref_sample_run(iters=1, threads=None):
 
 
 def cpu_baseline(args):
-    res = ref_sample_run(1)
+    res = ref_sample_run(workload(args), 1)
     if res is None:
         return {"value": None, "unit": "voxel-updates/s", "cores": 0, "kind": "reference",
                 "sample": "oracle/_ref not built"}
     v, dt, vox, thr, _ = res
     return {"value": v, "unit": "voxel-updates/s", "cores": thr, "kind": "reference",
             "sample": f"reference XT_Engine routines (updateVoxelsTimeSlices, iteration 1) on the same workload "
-                      f"restricted to a central disk of radius 64 voxels: {vox} voxel updates in {dt:.1f} s, "
+                      f"restricted to a central disk of radius {workload(args)['N'] // 8} voxels: {vox} voxel updates in {dt:.1f} s, "
                       f"OpenMP {thr} threads"}
 
 
@@ -299,7 +422,7 @@ def run_reference(args):
         return
     vals, tot = [], 0.0
     for s in range(args.warmup + args.steps):
-        res = ref_sample_run(1)
+        res = ref_sample_run(workload(args), 1)
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference build) missing"}))
             return
@@ -312,7 +435,9 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (same seeded workload, central-disk sample)",
-            "config": {"workload": "plain3d_512x512x64_1024views", "sample": "radius_obj 64 (1/16 of columns)"},
+            "config": dict(base_config(workload(args), args.amode),
+                           sample=f"radius_obj {workload(args)['N'] // 8} (about 1/20 of the columns)",
+                           parallelism="cpu"),
             "cpu_baseline": {"value": value, "unit": "voxel-updates/s", "cores": thr, "kind": "reference",
                              "sample": "one reference iteration per step on the central-disk sample"},
             "e2e": {"value": value, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -329,7 +454,13 @@ def main():
                     help="A storage: table32 (exact FP32 column table), fp16 (FP16 column table), "
                          "fp32 (computed at every column visit)")
     ap.add_argument("--columns", type=int, default=0)
+    ap.add_argument("--workload", default="plain3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--nxy", type=int, default=0,
+                    help="voxels per side (= detector bins) instead of the workload's; for profiling captures")
+    ap.add_argument("--zslab", type=int, default=0,
+                    help="z slices per ICD work piece (0: chosen from the L2 size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-converge", action="store_true", help="skip the seconds-to-converged-cost run")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

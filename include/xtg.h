@@ -50,8 +50,10 @@ enum {
  *   XTG_A_TABLE32: the same FP32 entries precomputed once per context into
  *                  an HBM column table (4 B offset + 4 B value per entry).
  *   XTG_A_FP16:    the column table with FP16 values and one FP32 scale per
- *                  (frame, column) -- the FP16-A precision form. */
-enum { XTG_A_FP32 = 0, XTG_A_FP16 = 1, XTG_A_TABLE32 = 2 };
+ *                  (frame, column) -- the FP16-A precision form.
+ *   XTG_A_AUTO:    xtg_set_options picks TABLE32 when the table fits in free
+ *                  device memory with 2 GiB to spare, else FP16, else FP32. */
+enum { XTG_A_FP32 = 0, XTG_A_FP16 = 1, XTG_A_TABLE32 = 2, XTG_A_AUTO = 3 };
 
 /* Update order.
  *   XTG_ORDER_PARALLEL: many columns in flight at once (the B200 schedule);
@@ -84,7 +86,8 @@ void xtg_destroy(xtg_ctx *ctx);
 const char *xtg_last_error(void);
 int xtg_abi_version(void);
 
-/* dims[]: N_x, N_y, N_z, N_time, N_r, N_t, N_p, nzb, zovl, amax */
+/* dims[11]: N_x, N_y, N_z, N_time, N_r, N_t, N_p, nzb, zovl, amax, and the
+ * number of x-y columns inside the reconstruction disk (radius_obj) */
 int xtg_dims(const xtg_ctx *ctx, int32_t *dims);
 /* Geometry and tables exactly as the GPU uses them (host copies). */
 int xtg_geometry(const xtg_ctx *ctx, xt_geom *g);
@@ -93,6 +96,14 @@ int xtg_get_hr(const xtg_ctx *ctx, float *hr /*[N_p][65]*/);
 /* Options: A storage, update order, concurrent columns (0 = device default),
  * seed of the GPU visiting order. */
 int xtg_set_options(xtg_ctx *ctx, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed);
+/* Parallel schedule: z slices per ICD work piece (0 = chosen from the L2 size,
+ * the default).  Each column visit is cut into pieces of at most this many
+ * slices, visited piece-major, so the error-sinogram and weight rows in
+ * flight fit in L2.  The sequential order always takes whole items.  No
+ * reference counterpart (a B200 scheduling knob). */
+int xtg_set_zslab(xtg_ctx *ctx, int32_t slices);
+/* The z slices per work piece the parallel schedule uses now. */
+int xtg_get_zslab(const xtg_ctx *ctx, int32_t *slices);
 
 /* genSinogram_fromBin + computeWriteSinogram (XT_genSinogram.c:264-300,
  * XT_Engine.c:89-121): y, w and the offset d (NULL = zero).  Weights are
@@ -196,8 +207,9 @@ int64_t xtg_device_bytes(const xtg_ctx *ctx);
 /* Kernel launches issued by this context since creation (all kernels). */
 int64_t xtg_launch_count(const xtg_ctx *ctx);
 /* Device time (ms) of the ICD column kernel in the last xtg_icd_iteration /
- * xtg_update_columns call, and the column work items it processed. */
-int xtg_last_kernel_time(const xtg_ctx *ctx, float *ms, int64_t *items, int64_t *rows_touched);
+ * xtg_update_columns call, the random-pass column work items it processed and
+ * the number of ICD kernel launches it issued. */
+int xtg_last_kernel_time(const xtg_ctx *ctx, float *ms, int64_t *items, int64_t *launches);
 
 #ifdef __cplusplus
 }

@@ -162,13 +162,18 @@ def converged_cost_fp64(name, iters=120):
     return o.cost()[0], o.object()
 
 
-@pytest.mark.parametrize("name,amode", [("plain3d", xtg.XTG_A_FP32), ("plain3d", xtg.XTG_A_FP16),
-                                        ("plain3d", xtg.XTG_A_TABLE32), ("zinger_nhicd", xtg.XTG_A_FP32),
-                                        ("zinger_nhicd", xtg.XTG_A_TABLE32), ("timbir4d", xtg.XTG_A_FP32),
-                                        ("timbir4d", xtg.XTG_A_FP16)])
-def test_parallel_icd_converges_to_oracle(name, amode):
+@pytest.mark.parametrize("name,amode,zslab", [("plain3d", xtg.XTG_A_FP32, 0), ("plain3d", xtg.XTG_A_FP16, 0),
+                                              ("plain3d", xtg.XTG_A_TABLE32, 0), ("zinger_nhicd", xtg.XTG_A_FP32, 0),
+                                              ("zinger_nhicd", xtg.XTG_A_TABLE32, 0), ("timbir4d", xtg.XTG_A_FP32, 0),
+                                              ("timbir4d", xtg.XTG_A_FP16, 0), ("plain3d", xtg.XTG_A_TABLE32, 2),
+                                              ("zinger_nhicd", xtg.XTG_A_TABLE32, 1), ("blocks_z", xtg.XTG_A_FP32, 4)])
+def test_parallel_icd_converges_to_oracle(name, amode, zslab):
+    """zslab > 0 cuts every column visit into z pieces of that many slices,
+    visited piece-major (the schedule large volumes use to keep e and w in L2)."""
     cstar, xstar = converged_cost_fp64(name)
     c, g, _ = ctx_for(name, a_mode=amode)
+    c.set_zslab(zslab)
+    assert c.zslab() == (zslab or c.N_z)
     c.upload_sino(g["y"], g["w"])
     c.init_error_sino()
     costs = []
@@ -215,3 +220,28 @@ def test_offset_and_variance_updates():
     o.update_variance()
     assert c.variance() == pytest.approx(o.var(), rel=1e-4)
     assert np.allclose(c.weight(), o.weight(), rtol=1e-4)
+
+
+@pytest.mark.parametrize("zslab", [1, 2, 3])
+def test_zslab_pieces_update_each_voxel_once(zslab):
+    """One column visit cut into z pieces: only that column changes, and its
+    MagUpdateMap entries hold the sum of |dx| over each z-block."""
+    c, g, p = ctx_for("blocks_z")
+    c.set_zslab(zslab)
+    c.upload_sino(g["y"], g["w"])
+    c.upload_object(g["objs"][0])
+    c.init_error_sino()
+    x0 = c.object()
+    st = c.update_columns(2, np.array([[0, 7, 9, -1]], np.int32))
+    assert st.columns == 1
+    dx = c.object() - x0
+    mask = np.zeros_like(dx, bool)
+    mask[0, :, 7, 9] = True
+    assert np.all(dx[~mask] == 0)
+    assert st.voxel_updates + st.zero_skipped == c.N_z
+    m = c.magmap()
+    zstep = c.N_z // c.nzb
+    for b in range(c.nzb):
+        z1 = c.N_z if b == c.nzb - 1 else (b + 1) * zstep
+        want = float(np.abs(dx[0, b * zstep:z1, 7, 9]).sum())
+        assert m[0, b, 7, 9] == pytest.approx(want, rel=1e-5, abs=1e-12)

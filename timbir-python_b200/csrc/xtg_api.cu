@@ -14,6 +14,7 @@
 //   k_offset_* / k_var_*   offset d and variance re-estimation
 //   k_build_items / k_magsum / k_build_a16 / k_counts / object transposes
 #include <algorithm>
+#include <numeric>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -82,12 +83,15 @@ struct xtg_ctx {
   int a_mode = XTG_A_FP32, order = XTG_ORDER_PARALLEL, max_columns = 0, span = 3;
   unsigned long long seed = 0x5eed5eedULL;
   int sm_count = 0;
+  long long l2_bytes = 0;
+  int zslab_req = 0;  // z slices per ICD work piece; 0 = from the L2 size
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
   int have_sino = 0;
   long long launches = 0;
   float last_kms = 0.f;
-  long long last_items = 0, last_rows = 0;
+  long long last_items = 0, last_icd = 0;
+  long long icd_launches = 0;  // ICD column-kernel launches since creation
   size_t dev_bytes = 0;
   // Park-Miller state for the reference-order mode (randlib.c:119-168)
   unsigned int sd[2] = {0, 0};
@@ -576,7 +580,14 @@ int xtg_create(const xt_params *prm, const double *times, const double *angles, 
   const xt_geom &g = c->g;
   c->G = make_devgeo(g, prm->positivity);
   c->sm_count = prop.multiProcessorCount;
+  c->l2_bytes = prop.l2CacheSize;
   c->ns = (size_t)g.N_p * g.N_r * g.N_t;
+  if (c->ns >= ((size_t)1 << 31)) {
+    // the kernels address the sinogram with 32-bit entry offsets
+    set_err("xtg_create: sinogram of %zu entries exceeds 2^31 - 1", c->ns);
+    xtg_destroy(c);
+    return XTG_E_ARG;
+  }
   c->nrt = (size_t)g.N_r * g.N_t;
   c->nxy = (size_t)g.N_x * g.N_y;
   c->nvox = (size_t)g.N_time * g.N_z * c->nxy;
@@ -660,7 +671,7 @@ int xtg_dims(const xtg_ctx *c, int32_t *d) {
   if (!c || !d) return XTG_E_ARG;
   const xt_geom &g = c->g;
   d[0] = g.N_x; d[1] = g.N_y; d[2] = g.N_z; d[3] = g.N_time; d[4] = g.N_r; d[5] = g.N_t; d[6] = g.N_p;
-  d[7] = g.nzb; d[8] = g.zovl; d[9] = g.amax;
+  d[7] = g.nzb; d[8] = g.zovl; d[9] = g.amax; d[10] = c->n_masked;
   return 0;
 }
 
@@ -676,11 +687,33 @@ int xtg_get_hr(const xtg_ctx *c, float *hr) {
   return 0;
 }
 
+static int choose_amode(xtg_ctx *c, int *mode);
+static int zslab(const xtg_ctx *c);
+
+int xtg_get_zslab(const xtg_ctx *c, int32_t *slices) {
+  if (!c || !slices) return XTG_E_ARG;
+  *slices = zslab(c);
+  return 0;
+}
+
+int xtg_set_zslab(xtg_ctx *c, int32_t slices) {
+  if (!c || slices < 0) {
+    set_err("xtg_set_zslab: bad argument");
+    return XTG_E_ARG;
+  }
+  c->zslab_req = slices;
+  return 0;
+}
+
 int xtg_set_options(xtg_ctx *c, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed) {
-  if (!c || (a_mode != XTG_A_FP32 && a_mode != XTG_A_FP16 && a_mode != XTG_A_TABLE32) ||
+  if (!c || (a_mode != XTG_A_FP32 && a_mode != XTG_A_FP16 && a_mode != XTG_A_TABLE32 && a_mode != XTG_A_AUTO) ||
       (order != XTG_ORDER_PARALLEL && order != XTG_ORDER_SEQUENTIAL) || max_columns < 0) {
     set_err("xtg_set_options: bad option");
     return XTG_E_ARG;
+  }
+  if (a_mode == XTG_A_AUTO) {
+    int rc = choose_amode(c, &a_mode);
+    if (rc) return rc;
   }
   if (a_mode != c->a_mode && c->table_mode != 0 && a_mode != XTG_A_FP32) {
     // the entry offsets are shared; only the value array differs between table types
@@ -984,16 +1017,23 @@ int xtg_update_variance(xtg_ctx *c) {
 // ------------------------------------------------------------ ICD driver --
 // Builds the A-matrix column table for the current a_mode (count pass, host
 // prefix sum, fill pass).  Rebuilt only when the value type changes.
-static int ensure_table(xtg_ctx *c) {
-  if (c->table_mode == c->a_mode) return 0;
-  const size_t ncol = (size_t)c->g.N_time * c->n_masked;
+static TableArgs table_args(const xtg_ctx *c) {
   TableArgs T;
   memset(&T, 0, sizeof(T));
   T.hr = c->d_hr; T.cosv = c->d_cos; T.sinv = c->d_sin; T.view_idx = c->d_view_idx; T.view_start = c->d_view_start;
   T.view_num = c->d_view_num; T.mcols = c->d_mcols; T.n_masked = c->n_masked;
+  return T;
+}
+
+// Entries per (frame, masked column) over the frame's views, turned into run
+// starts on the host; returns the total and the longest run.
+static int count_table(xtg_ctx *c, std::vector<long long> &cnt, long long *total, long long *longest) {
+  const size_t ncol = (size_t)c->g.N_time * c->n_masked;
+  TableArgs T = table_args(c);
   if (!c->d_tstart && dalloc(c, &c->d_tstart, ncol + 1)) return XTG_E_CUDA;
   CK(launch_table_count(c->G, T, c->span, c->d_tstart, c->st));
-  std::vector<long long> cnt(ncol + 1, 0);
+  c->launches++;
+  cnt.assign(ncol + 1, 0);
   CK(cudaMemcpyAsync(cnt.data(), c->d_tstart, ncol * 8, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   long long run = 0, mx = 0;
@@ -1004,6 +1044,38 @@ static int ensure_table(xtg_ctx *c) {
     mx = std::max(mx, n);
   }
   cnt[ncol] = run;
+  *total = run;
+  *longest = mx;
+  return 0;
+}
+
+// XTG_A_AUTO: the exact FP32 table when it fits in free device memory with
+// 2 GiB to spare, else the FP16 table, else entries computed per visit.
+static int choose_amode(xtg_ctx *c, int *mode) {
+  std::vector<long long> cnt;
+  long long run = 0, mx = 0;
+  int rc = count_table(c, cnt, &run, &mx);
+  if (rc) return rc;
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const size_t reserve = (size_t)2 << 30, ncol = (size_t)c->g.N_time * c->n_masked;
+  if ((size_t)run * 8 + reserve < fr)
+    *mode = XTG_A_TABLE32;
+  else if ((size_t)run * 6 + ncol * 4 + reserve < fr)
+    *mode = XTG_A_FP16;
+  else
+    *mode = XTG_A_FP32;
+  return 0;
+}
+
+static int ensure_table(xtg_ctx *c) {
+  if (c->table_mode == c->a_mode) return 0;
+  const size_t ncol = (size_t)c->g.N_time * c->n_masked;
+  TableArgs T = table_args(c);
+  std::vector<long long> cnt;
+  long long run = 0, mx = 0;
+  int rc = count_table(c, cnt, &run, &mx);
+  if (rc) return rc;
   if (c->d_toff && c->table_nnz != run) {
     set_err("A table size changed");
     return XTG_E_STATE;
@@ -1025,9 +1097,31 @@ static int ensure_table(xtg_ctx *c) {
   T.off = c->d_toff;
   CK(launch_table_fill(c->G, T, c->span, c->st));
   CK(cudaStreamSynchronize(c->st));
-  c->launches += 2;
+  c->launches++;
   c->table_mode = c->a_mode;
   return 0;
+}
+
+// z slices per ICD work piece.  Whole z-lines by default: every piece
+// restages the column's A entries, so on the plain-3D-at-scale workload
+// (512^2 x 64) pieces sized to keep the e and w rows in flight inside L2
+// (16 slices) ran 19 % slower than whole lines.  Lines longer than the
+// kernel's row limit (128 detector rows with 16-byte access, else 32) are cut
+// into equal pieces whose rows keep 16-byte alignment.
+static int zslab(const xtg_ctx *c) {
+  const xt_geom &g = c->g;
+  if (c->zslab_req > 0) return std::min(c->zslab_req, g.N_z);
+  const int max_rows = (g.N_t % 4 == 0) ? 128 : 32;
+  const int fit = std::max(1, max_rows / g.zovl);
+  if (g.N_z <= fit) return g.N_z;
+  const int npiece = (g.N_z + fit - 1) / fit;
+  int hz = (g.N_z + npiece - 1) / npiece;
+  if (g.N_t % 4 == 0) {
+    const int q = 4 / std::gcd(4, g.zovl);  // slices per 4 rows
+    hz = (hz + q - 1) / q * q;
+    if (hz > fit) hz = fit / q * q;
+  }
+  return std::max(1, hz);
 }
 
 // one ICD launch over items[lo, lo+n) (or a device-counted list)
@@ -1039,15 +1133,29 @@ static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, c
     if (rc) return rc;
   }
   const int seq = (seq_override >= 0) ? seq_override : (c->order == XTG_ORDER_SEQUENTIAL);
-  // rows of the largest work item: a whole z-line, or one z-block (the last
-  // block is the longest); shared memory is sized for it
+  // slices of the largest work item: a whole z-line, or one z-block (the
+  // last block is the longest)
   const int last_block = g.N_z - (g.nzb - 1) * g.zstep;
-  const int zmax = has_whole ? g.N_z : last_block;
+  const int zitem = has_whole ? g.N_z : last_block;
+  // the parallel schedule splits items into z pieces of at most hz slices
+  // and visits them piece-major; shared memory is sized for one piece
+  const int hz = seq ? zitem : std::min(zitem, zslab(c));
+  const int nsub = (zitem + hz - 1) / hz;
+  const int zmax = hz;
   const int rows = zmax * g.zovl;
-  // 16-byte vector access needs every item's first row and row count to be
-  // multiples of 4 (the last block's rows too)
+  // 16-byte vector access needs every piece's first row and row count to be
+  // multiples of 4
   bool v4 = (g.N_t % 4 == 0);
-  if (has_blocks) v4 = v4 && ((g.zstep * g.zovl) % 4 == 0) && ((last_block * g.zovl) % 4 == 0);
+  auto pieces_ok = [&](int z0, int len) {
+    for (int o = 0; o < len; o += hz) {
+      const int l = std::min(hz, len - o);
+      if (((z0 + o) * g.zovl) % 4 || (l * g.zovl) % 4) return false;
+    }
+    return true;
+  };
+  if (has_whole) v4 = v4 && pieces_ok(0, g.N_z);
+  if (has_blocks)
+    for (int b = 0; b < g.nzb && v4; b++) v4 = pieces_ok(b * g.zstep, b == g.nzb - 1 ? last_block : g.zstep);
   const int vec = v4 ? 4 : 1;
   if ((rows + vec - 1) / vec > 32) {
     set_err("ICD work item of %d detector rows exceeds the kernel's %d (N_z/nzb too large)", rows, 32 * vec);
@@ -1070,6 +1178,11 @@ static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, c
   A.use_perm = use_perm; A.perm_key = key; A.col_rank = c->d_rank; A.n_masked = c->n_masked; A.iter = iter;
   A.tstart = c->d_tstart; A.toff = c->d_toff; A.tval32 = c->d_tval32; A.tval16 = c->d_tval16; A.tscale = c->d_tscale;
   A.T2 = g.T * g.T; A.Tdelta = g.T * g.delta; A.st_absx = c->d_absx; A.st_cnt = c->d_cnt; A.err = c->d_err;
+  A.zslab = hz; A.nsub = nsub;
+  if (nsub > 1) {
+    CK(launch_magmap_zero(c->G, A, c->sm_count * 4, c->st));
+    c->launches++;
+  }
   int grid;
   if (seq) {
     grid = 1;
@@ -1077,10 +1190,11 @@ static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, c
     const int occ = icd_occupancy(vec, amode, 0, as, vcap, zmax, g.zovl);
     grid = c->sm_count * occ;
     if (c->max_columns > 0) grid = std::min(grid, c->max_columns);
-    if (!n_dev) grid = std::min(grid, std::max(n, 1));
+    if (!n_dev) grid = std::min(grid, std::max(n * nsub, 1));
   }
   CK(cudaMemsetAsync(c->d_counter, 0, 4, c->st));
   CK(launch_icd(c->G, A, vec, amode, seq, as, vcap, zmax, grid, c->st));
+  c->icd_launches++;
   c->launches++;
   return 0;
 }
@@ -1194,6 +1308,7 @@ static float host_randomized_select(xtg_ctx *c, float *A, unsigned p, unsigned r
 }
 
 static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
+  const long long icd0 = c->icd_launches;
   const xt_geom &g = c->g;
   const int n = g.N_time * c->n_masked;
   const unsigned long long key = c->seed * 0x9E3779B97F4A7C15ULL + (unsigned long long)iter * 0xD1B54A32D192ED03ULL;
@@ -1259,11 +1374,13 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
   if (rc) return rc;
   c->last_kms = kms_total;
   c->last_items = items_total;
+  c->last_icd = c->icd_launches - icd0;
   st->vox_mag = vox_mag;
   return 0;
 }
 
 static int icd_iteration_sequential(xtg_ctx *c, int iter, xtg_stats *st) {
+  const long long icd0 = c->icd_launches;
   const xt_geom &g = c->g;
   const int nxy = (int)c->nxy, K = XT_NHICD_CHUNKS;
   std::vector<int> usn, xs, ys;
@@ -1375,6 +1492,7 @@ static int icd_iteration_sequential(xtg_ctx *c, int iter, xtg_stats *st) {
   if (rc) return rc;
   c->last_kms = kms_total;
   c->last_items = items_total;
+  c->last_icd = c->icd_launches - icd0;
   st->vox_mag = vox_mag;
   return 0;
 }
@@ -1418,6 +1536,8 @@ int xtg_icd_iteration(xtg_ctx *c, int32_t iter, xtg_stats *st_out) {
 }
 
 int xtg_update_columns(xtg_ctx *c, int32_t iter, int32_t n, const int32_t *items, xtg_stats *st_out) {
+  if (!c) return XTG_E_ARG;
+  const long long icd0 = c->icd_launches;
   if (!c || n < 0 || (n && !items)) return XTG_E_ARG;
   if (!c->have_sino) {
     set_err("xtg_update_columns: no sinogram uploaded");
@@ -1457,6 +1577,7 @@ int xtg_update_columns(xtg_ctx *c, int32_t iter, int32_t n, const int32_t *items
   st.vox_mag = ab;
   c->last_kms = st.ms;
   c->last_items = n;
+  c->last_icd = c->icd_launches - icd0;
   rc = check_err_flag(c);
   if (rc) return rc;
   if (st_out) *st_out = st;
@@ -1503,11 +1624,11 @@ int xtg_nhicd_select(xtg_ctx *c, const int32_t *usn, int32_t *nnum, int32_t *xse
 int64_t xtg_device_bytes(const xtg_ctx *c) { return c ? (int64_t)c->dev_bytes : 0; }
 int64_t xtg_launch_count(const xtg_ctx *c) { return c ? (int64_t)c->launches : 0; }
 
-int xtg_last_kernel_time(const xtg_ctx *c, float *ms, int64_t *items, int64_t *rows) {
+int xtg_last_kernel_time(const xtg_ctx *c, float *ms, int64_t *items, int64_t *launches) {
   if (!c) return XTG_E_ARG;
   if (ms) *ms = c->last_kms;
   if (items) *items = c->last_items;
-  if (rows) *rows = c->last_rows;
+  if (launches) *launches = c->last_icd;
   return 0;
 }
 

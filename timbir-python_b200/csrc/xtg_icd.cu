@@ -65,10 +65,10 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
   int *sPack = reinterpret_cast<int *>(smem_raw);        // [vmax]
   int *sView = sPack + vmax;                              // [vmax]
   float *sVal = reinterpret_cast<float *>(sView + vmax);  // [AS][vmax] A * delta_t
-  // AMODE 1/2 (column table): the column's entry run, vmax = longest run
-  int *sOff = reinterpret_cast<int *>(smem_raw);         // [vmax] (p*N_r + bin)*N_t
-  float *sA = reinterpret_cast<float *>(sOff + vmax);    // [vmax] A * delta_t
-  float *sRed = (AMODE == 0) ? sVal + (size_t)vmax * AS : sA + vmax;  // [2][8][128] warp partials
+  // AMODE 1/2 (column table): the column's entry run, vmax = longest run,
+  // {(p*N_r + bin)*N_t, bits of A * delta_t} per entry (one 8-byte load)
+  int2 *sEnt = reinterpret_cast<int2 *>(smem_raw);       // [vmax]
+  float *sRed = (AMODE == 0) ? sVal + (size_t)vmax * AS : reinterpret_cast<float *>(sEnt + vmax);  // [2][8][128]
   float *sTh = sRed + 2 * 8 * 128;                        // [2][zmax*zovl]
   const int rowsmax = zmax * G.zovl;
   float *sNb = sTh + 2 * rowsmax;                         // [9][zmax+2]
@@ -89,8 +89,9 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     }
     __syncthreads();
     const int it = sItem;
-    if (it >= nitems) break;
-    const int q = A.use_perm ? (int)xt_perm((uint32_t)it, (uint32_t)nitems, A.perm_key) : it;
+    if (it >= nitems * A.nsub) break;
+    const int piece = it / nitems, ii = it - piece * nitems;
+    const int q = A.use_perm ? (int)xt_perm((uint32_t)ii, (uint32_t)nitems, A.perm_key) : ii;
     const int4 item = A.items[A.item_lo + q];
     const int fr = item.x, row = item.y, col = item.z, blk = item.w;
     int zb = 0, ze = G.N_z - 1;
@@ -98,35 +99,16 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
       zb = blk * G.zstep;
       ze = (blk >= G.nzb - 1) ? G.N_z - 1 : (blk + 1) * G.zstep - 1;
     }
+    zb += piece * A.zslab;
+    if (zb > ze) {  // this item has fewer pieces (uniform over the CTA)
+      __syncthreads();
+      continue;
+    }
+    ze = min(ze, zb + A.zslab - 1);
     const int Z = ze - zb + 1, T = Z * G.zovl, t0 = zb * G.zovl;
     const int V = A.view_num[fr], vs = A.view_start[fr];
 
-    // 1. the column's A entries (times delta_t, XT_VoxUpdate.c:27) -> smem
-    if (AMODE == 0) {
-      for (int v = tid; v < V; v += XTG_THREADS) {
-        const int p = A.view_idx[vs + v];
-        float vals[AS];
-        int first;
-        const int n = xt_amatrix_regs<AS>(G, A.hr + (size_t)p * XT_HR_STRIDE, A.cosv[p], A.sinv[p], row, col, vals,
-                                          &first);
-        sPack[v] = first | (n << 24);
-        sView[v] = p;
-#pragma unroll
-        for (int s = 0; s < AS; s++) sVal[s * vmax + v] = __fmul_rn(vals[s], G.delta_t);
-      }
-    }
-    int ne = 0;
-    if (AMODE != 0) {
-      const long long ti = (long long)fr * A.n_masked + A.col_rank[row * G.N_x + col];
-      const long long s0 = A.tstart[ti];
-      ne = (int)(A.tstart[ti + 1] - s0);
-      const float sc = (AMODE == 1) ? A.tscale[ti] : 1.f;
-      for (int e = tid; e < ne; e += XTG_THREADS) {
-        sOff[e] = __ldg(A.toff + s0 + e);
-        sA[e] = (AMODE == 2) ? __ldg(A.tval32 + s0 + e) : __half2float(A.tval16[s0 + e]) * sc;
-      }
-    }
-    // 2. neighbourhood: the 3x3 columns' z-lines over [zb-1, ze+1], and the
+    // 1. neighbourhood: the 3x3 columns' z-lines over [zb-1, ze+1], and the
     //    same column in frames fr-1 and fr+1 (0 outside the volume)
     const size_t plane = (size_t)G.N_y * G.N_x;
     for (int k = tid; k < 9 * (Z + 2); k += XTG_THREADS) {
@@ -143,6 +125,49 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
       if (f2 >= 0 && f2 < G.N_time) v = A.x[(((size_t)f2 * plane) + (size_t)row * G.N_x + col) * G.N_z + zb + z];
       sTn[s * zmax + z] = v;
     }
+    // Zero skipping (XT_VoxUpdate.c:208-232) decided for the whole z-line
+    // before any footprint work: from the second iteration a voxel equal to 0
+    // with no positive spatial or temporal neighbour is not updated.  When
+    // that holds for every voxel of the item, theta is never used, so neither
+    // A nor the footprint is read (the update step below skips each voxel by
+    // the same test and the e update has nothing to add).
+    bool quiet = A.iter > 1;
+    if (quiet) {
+      for (int k = tid; k < 9 * (Z + 2); k += XTG_THREADS) {
+        const int c = k / (Z + 2), zz = k - c * (Z + 2);
+        const float v = sNb[c * (zmax + 2) + zz];
+        const bool self = (c == 4) && zz >= 1 && zz <= Z;
+        if (self ? (v != 0.f) : (v > 0.f)) quiet = false;
+      }
+      for (int k = tid; k < 2 * Z; k += XTG_THREADS)
+        if (sTn[(k / Z) * zmax + k % Z] > 0.f) quiet = false;
+    }
+    const bool skip_all = __syncthreads_and(quiet) != 0;
+    // 2. the column's A entries (times delta_t, XT_VoxUpdate.c:27) -> smem
+    if (AMODE == 0 && !skip_all) {
+      for (int v = tid; v < V; v += XTG_THREADS) {
+        const int p = A.view_idx[vs + v];
+        float vals[AS];
+        int first;
+        const int n = xt_amatrix_regs<AS>(G, A.hr + (size_t)p * XT_HR_STRIDE, A.cosv[p], A.sinv[p], row, col, vals,
+                                          &first);
+        sPack[v] = first | (n << 24);
+        sView[v] = p;
+#pragma unroll
+        for (int s = 0; s < AS; s++) sVal[s * vmax + v] = __fmul_rn(vals[s], G.delta_t);
+      }
+    }
+    int ne = 0;
+    if (AMODE != 0 && !skip_all) {
+      const long long ti = (long long)fr * A.n_masked + A.col_rank[row * G.N_x + col];
+      const long long s0 = A.tstart[ti];
+      ne = (int)(A.tstart[ti + 1] - s0);
+      const float sc = (AMODE == 1) ? A.tscale[ti] : 1.f;
+      for (int e = tid; e < ne; e += XTG_THREADS) {
+        const float a = (AMODE == 2) ? __ldg(A.tval32 + s0 + e) : __half2float(A.tval16[s0 + e]) * sc;
+        sEnt[e] = make_int2(__ldg(A.toff + s0 + e), __float_as_int(a));
+      }
+    }
     __syncthreads();
 
     // 3. theta1 / theta2 over the column's footprint (XT_VoxUpdate.c:20-51)
@@ -153,60 +178,74 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     float th1[VEC], th2[VEC];
 #pragma unroll
     for (int c = 0; c < VEC; c++) th1[c] = th2[c] = 0.f;
-    // one footprint entry: rows [base, base + VEC) of one (view, bin), weight a
-    auto accumulate = [&](size_t base, float a) {
-      const float a2 = a * a;
+    // one footprint entry: rows [off, off + VEC) past this thread's first row
+    // of one (view, bin), weight a.  Generalized-Huber (zinger) weight
+    // (XT_VoxUpdate.c:34-48): w where |e sqrt(w)| < T, else
+    // we = T delta sqrt(w) / |e|, so that
+    //   theta2 += a^2 we = a^2 T delta sqrt(w) / |e|,
+    //   theta1 -= a e we = a T delta sign(e) sqrt(w);
+    // sqrt(w) = w rsqrt(w) and 1/|e| come from the special-function unit, and
+    // the branch runs only when some lane of the warp meets a zinger.
+    const int trow0 = t0 + tl * VEC;
+    const float *eb = A.e + trow0;
+    const float *wb = A.w + trow0;
+    auto accumulate = [&](int off, float a) {
+      const float a2 = a * a, na = -a;
       float ev[VEC], wv[VEC];
       if (VEC == 4) {
-        const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(A.e + base));
-        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(A.w + base));
+        const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(eb + off));
+        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wb + off));
         ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
         wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
       } else {
 #pragma unroll
         for (int c = 0; c < VEC; c++) {
-          ev[c] = __ldcg(A.e + base + c);
-          wv[c] = __ldg(A.w + base + c);
+          ev[c] = __ldcg(eb + off + c);
+          wv[c] = __ldg(wb + off + c);
         }
       }
-      // generalized-Huber (zinger) weight: w where |e sqrt(w)| < T, else
-      // T delta sqrt(w) / |e| (XT_VoxUpdate.c:34-48); the slow branch runs
-      // only when some lane of the warp needs it
-      float ew[VEC];
-      bool zg = false;
+      float ew[VEC], q[VEC];
+      float qm = 0.f;
 #pragma unroll
       for (int c = 0; c < VEC; c++) {
         ew[c] = ev[c] * wv[c];
-        zg |= (ev[c] * ew[c] >= A.T2);
+        q[c] = ev[c] * ew[c];  // e^2 w
+        qm = fmaxf(qm, q[c]);
       }
-      if (__any_sync(__activemask(), zg)) {
+      if (__any_sync(__activemask(), qm >= A.T2)) {
 #pragma unroll
         for (int c = 0; c < VEC; c++) {
-          float we = wv[c];
-          if (ev[c] * ew[c] >= A.T2) we = __fdividef(A.Tdelta * sqrtf(wv[c]), fabsf(ev[c]));
-          th2[c] = fmaf(a2, we, th2[c]);
-          th1[c] = fmaf(-a * ev[c], we, th1[c]);
+          if (q[c] >= A.T2) {
+            const float sw = wv[c] * rsqrtf(wv[c]);
+            th2[c] = fmaf(a2 * A.Tdelta, __fdividef(sw, fabsf(ev[c])), th2[c]);
+            th1[c] = fmaf(na * A.Tdelta, copysignf(sw, ev[c]), th1[c]);
+          } else {
+            th2[c] = fmaf(a2, wv[c], th2[c]);
+            th1[c] = fmaf(na, ew[c], th1[c]);
+          }
         }
       } else {
 #pragma unroll
         for (int c = 0; c < VEC; c++) {
           th2[c] = fmaf(a2, wv[c], th2[c]);
-          th1[c] = fmaf(-a, ew[c], th1[c]);
+          th1[c] = fmaf(na, ew[c], th1[c]);
         }
       }
     };
-    if (tl < tln) {
-      const int trow = t0 + tl * VEC;
+    if (tl < tln && !skip_all) {
       if (AMODE == 0) {
         for (int v = vg; v < V; v += vgs) {
           const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
-          const size_t base = ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
+          const int off = (sView[v] * G.N_r + first) * G.N_t;
 #pragma unroll
           for (int s = 0; s < AS; s++)
-            if (s < n) accumulate(base + (size_t)s * G.N_t, sVal[s * vmax + v]);
+            if (s < n) accumulate(off + s * G.N_t, sVal[s * vmax + v]);
         }
       } else {
-        for (int e = vg; e < ne; e += vgs) accumulate((size_t)sOff[e] + trow, sA[e]);
+        for (int e = vg; e < ne; e += vgs) {
+          const int2 en = sEnt[e];
+          accumulate(en.x, __int_as_float(en.y));
+        }
       }
     }
     // reduce over view groups: lanes with equal tl inside a warp, then warps
@@ -358,10 +397,19 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     //    slices of this visit (XT_VoxUpdate.c:128, 236); sum |x| and counters
     for (int b = tid; b < G.nzb; b += XTG_THREADS) {
       const int bz0 = b * G.zstep, bz1 = (b >= G.nzb - 1) ? G.N_z - 1 : (b + 1) * G.zstep - 1;
-      if (bz0 >= zb && bz1 <= ze) {
+      const int lo = max(bz0, zb), hi = min(bz1, ze);
+      float *mp = A.magmap + (((size_t)fr * G.nzb + b) * G.N_y + row) * G.N_x + col;
+      if (A.nsub > 1) {
+        // pieces of one block add into the entry zeroed before the launch
+        if (lo <= hi) {
+          float m = 0.f;
+          for (int z = lo; z <= hi; z++) m += fabsf(sDelta[z - zb]);
+          atomicAdd(mp, m);
+        }
+      } else if (bz0 >= zb && bz1 <= ze) {
         float m = 0.f;
         for (int z = bz0; z <= bz1; z++) m += fabsf(sDelta[z - zb]);
-        A.magmap[(((size_t)fr * G.nzb + b) * G.N_y + row) * G.N_x + col] = m;
+        *mp = m;
       }
     }
     for (int off = 16; off > 0; off >>= 1) absx += __shfl_xor_sync(0xffffffffu, absx, off);
@@ -373,7 +421,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
       atomicAdd(&A.st_absx[blockIdx.x & 63], s);
       atomicAdd(&A.st_cnt[0], (unsigned long long)sUpd);
       atomicAdd(&A.st_cnt[1], (unsigned long long)sZero);
-      atomicAdd(&A.st_cnt[2], 1ull);
+      if (piece == 0) atomicAdd(&A.st_cnt[2], 1ull);
     }
 
     // 6. e -= (A delta_t) * delta_x on the footprint (XT_VoxUpdate.c:62-82)
@@ -387,26 +435,29 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
         any |= (dv[c] != 0.f);
       }
       if (any) {
-        const int trow = t0 + tl * VEC;
-        auto scatter = [&](float *ep, float a) {
+        float *ebw = A.e + trow0;
+        auto scatter = [&](int off, float a) {
           if (VEC == 4) {
-            xt_red_add4(ep, -(a * dv[0]), -(a * dv[1]), -(a * dv[2]), -(a * dv[3]));
+            xt_red_add4(ebw + off, -(a * dv[0]), -(a * dv[1]), -(a * dv[2]), -(a * dv[3]));
           } else {
 #pragma unroll
             for (int c = 0; c < VEC; c++)
-              if (dv[c] != 0.f) atomicAdd(ep + c, -(a * dv[c]));
+              if (dv[c] != 0.f) atomicAdd(ebw + off + c, -(a * dv[c]));
           }
         };
         if (AMODE == 0) {
           for (int v = vg; v < V; v += vgs) {
             const int pk = sPack[v], first = pk & 0xffffff, n = pk >> 24;
-            float *ep = A.e + ((size_t)sView[v] * G.N_r + first) * G.N_t + trow;
+            const int off = (sView[v] * G.N_r + first) * G.N_t;
 #pragma unroll
             for (int s = 0; s < AS; s++)
-              if (s < n) scatter(ep + (size_t)s * G.N_t, sVal[s * vmax + v]);
+              if (s < n) scatter(off + s * G.N_t, sVal[s * vmax + v]);
           }
         } else {
-          for (int e = vg; e < ne; e += vgs) scatter(A.e + (size_t)sOff[e] + trow, sA[e]);
+          for (int e = vg; e < ne; e += vgs) {
+            const int2 en = sEnt[e];
+            scatter(en.x, __int_as_float(en.y));
+          }
         }
       }
     }
@@ -419,7 +470,7 @@ size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode) {
   if (amode == 0)
     b += (size_t)vmax * (4 * 2 + 4 * (size_t)as);  // sPack, sView, sVal
   else
-    b += (size_t)vmax * 8;                         // sOff, sA (vmax = longest column run)
+    b += (size_t)vmax * 8;                         // sEnt (vmax = longest column run)
   b += 2 * 8 * 128 * 4;                            // sRed
   b += 2 * (size_t)zmax * zovl * 4;                // sTh
   b += 9 * (size_t)(zmax + 2) * 4;                 // sNb
@@ -446,6 +497,25 @@ static IcdKernel icd_kernel(int vec, int amode, int seq, int as) {
   return seq ? XTG_T(1, 2, 1) : XTG_T(1, 2, 0);
 #undef XTG_K
 #undef XTG_T
+}
+
+// Zeroes MagUpdateMap[frame][block][row][col] for every (item, block the
+// item covers) of an ICD launch whose items are split into z pieces, which
+// then add their partial sums into it.
+__global__ void k_magmap_zero(DevGeo G, IcdArgs A) {
+  const int nitems = A.n_items_dev ? *A.n_items_dev : A.n_items;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nitems; i += gridDim.x * blockDim.x) {
+    const int q = A.use_perm ? (int)xt_perm((uint32_t)i, (uint32_t)nitems, A.perm_key) : i;
+    const int4 item = A.items[A.item_lo + q];
+    const int b0 = item.w >= 0 ? item.w : 0, b1 = item.w >= 0 ? item.w : G.nzb - 1;
+    for (int b = b0; b <= b1; b++)
+      A.magmap[(((size_t)item.x * G.nzb + b) * G.N_y + item.y) * G.N_x + item.z] = 0.f;
+  }
+}
+
+cudaError_t launch_magmap_zero(const DevGeo &G, const IcdArgs &A, int grid, cudaStream_t st) {
+  k_magmap_zero<<<grid, 256, 0, st>>>(G, A);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,

@@ -18,6 +18,10 @@ struct IcdArgs {
   int *counter;
   int use_perm;
   unsigned long long perm_key;
+  // z-slab split: base item i is processed as nsub pieces of at most zslab
+  // slices; the launch visits piece-major (all items' piece 0, then piece 1,
+  // ...), so the detector rows in flight stay within one slab of e and w
+  int zslab, nsub;
   // A column table (a_mode FP16 / FP32 table): entries of (frame, masked
   // column rank) at [tstart[i], tstart[i+1]), i = frame * n_masked + rank
   const long long *tstart;
@@ -62,6 +66,7 @@ cudaError_t launch_table_count(const DevGeo &G, const TableArgs &T, int ns, long
 cudaError_t launch_table_fill(const DevGeo &G, const TableArgs &T, int ns, cudaStream_t st);
 
 size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode);
+cudaError_t launch_magmap_zero(const DevGeo &G, const IcdArgs &A, int grid, cudaStream_t st);
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st);
 int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl);

@@ -252,13 +252,13 @@ int main(int argc, char **argv) {
     fprintf(stderr, "ERROR: %s\n", xtg_last_error());
     return 1;
   }
-  rc = xtg_set_options(ctx, O.a_fp16 ? XTG_A_FP16 : XTG_A_FP32, O.sequential ? XTG_ORDER_SEQUENTIAL : XTG_ORDER_PARALLEL,
+  rc = xtg_set_options(ctx, O.a_mode, O.sequential ? XTG_ORDER_SEQUENTIAL : XTG_ORDER_PARALLEL,
                        O.columns, O.seed);
   if (rc) {
     logf_("ERROR: %s\n", xtg_last_error());
     return 1;
   }
-  int32_t dims[10];
+  int32_t dims[11];
   xtg_dims(ctx, dims);
   const int N_x = dims[0], N_y = dims[1], N_z = dims[2], N_time = dims[3], N_r = dims[4], N_t = dims[5];
   const int N_p = dims[6], nzb = dims[7];
@@ -391,7 +391,7 @@ int main(int argc, char **argv) {
     if (O.resync_every > 0 && Iter % O.resync_every == 0)
       rc = xtg_resync_fp64(ctx, &cost, &fwd, &prior);
     else
-      rc = xtg_map_cost_fp64(ctx, &cost, &fwd, &prior);
+      rc = xtg_map_cost_running(ctx, &cost, &fwd, &prior);
     if (rc) {
       logf_("ERROR: %s\n", xtg_last_error());
       return 1;

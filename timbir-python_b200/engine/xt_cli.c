@@ -3,13 +3,14 @@
  */
 #define _GNU_SOURCE
 #include "xt_cli.h"
+#include "xtg.h"
 
 #include <getopt.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
-enum { OPT_POS = 300, OPT_DOUBLE, OPT_AFP16, OPT_SEQ, OPT_COLS, OPT_SEED, OPT_RESYNC, OPT_QUIET, OPT_HELP };
+enum { OPT_POS = 300, OPT_DOUBLE, OPT_AFP16, OPT_SEQ, OPT_COLS, OPT_SEED, OPT_RESYNC, OPT_QUIET, OPT_HELP, OPT_AMODE };
 
 int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
   /* option table of XT_Init.c:457-506: names, letters and argument kinds */
@@ -64,6 +65,7 @@ int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
       {"positivity", required_argument, 0, OPT_POS},
       {"real_is_double", no_argument, 0, OPT_DOUBLE},
       {"gpu_afp16", no_argument, 0, OPT_AFP16},
+      {"gpu_amode", required_argument, 0, OPT_AMODE},
       {"gpu_sequential", no_argument, 0, OPT_SEQ},
       {"gpu_columns", required_argument, 0, OPT_COLS},
       {"gpu_seed", required_argument, 0, OPT_SEED},
@@ -74,7 +76,8 @@ int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
   xt_params_default(p);
   memset(o, 0, sizeof(*o));
   o->seed = 761521;
-  o->resync_every = 1;
+  o->a_mode = XTG_A_AUTO;
+  o->resync_every = 10;
   optind = 0;
   for (;;) {
     int idx = 0;
@@ -130,7 +133,14 @@ int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
       case ']': p->x_width = atoi(optarg); break;
       case OPT_POS: p->positivity = atoi(optarg) != 0; break;
       case OPT_DOUBLE: p->real_is_double = 1; break;
-      case OPT_AFP16: o->a_fp16 = 1; break;
+      case OPT_AFP16: o->a_mode = XTG_A_FP16; break;
+      case OPT_AMODE:
+        if (!strcmp(optarg, "fp32")) o->a_mode = XTG_A_FP32;
+        else if (!strcmp(optarg, "table32")) o->a_mode = XTG_A_TABLE32;
+        else if (!strcmp(optarg, "fp16")) o->a_mode = XTG_A_FP16;
+        else if (!strcmp(optarg, "auto")) o->a_mode = XTG_A_AUTO;
+        else printf("ERROR: XT_Engine: --gpu_amode takes fp32, table32, fp16 or auto; keeping the default\n");
+        break;
       case OPT_SEQ: o->sequential = 1; break;
       case OPT_COLS: o->columns = atoi(optarg); break;
       case OPT_SEED: o->seed = strtoull(optarg, NULL, 10); break;
@@ -138,7 +148,8 @@ int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
       case OPT_QUIET: o->quiet = 1; break;
       case OPT_HELP:
         printf("XT_Engine: TIMBIR/MBIR reconstruction on one B200; options as the reference XT_Engine,\n"
-               "plus --positivity 0|1 --real_is_double --gpu_afp16 --gpu_sequential --gpu_columns N\n"
+               "plus --positivity 0|1 --real_is_double --gpu_amode fp32|table32|fp16|auto --gpu_afp16\n"
+               "--gpu_sequential --gpu_columns N\n"
                "--gpu_seed S --gpu_resync K --quiet\n");
         return 1;
       default:

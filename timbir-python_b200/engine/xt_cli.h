@@ -14,11 +14,12 @@
 #include "xt_geom.h"
 
 typedef struct {
-  int32_t a_fp16;       /* --gpu_afp16: FP16 A-matrix storage */
+  int32_t a_mode;       /* --gpu_amode fp32|table32|fp16|auto (XTG_A_*); --gpu_afp16 = fp16 */
   int32_t sequential;   /* --gpu_sequential: reference visiting order, one column at a time */
   int32_t columns;      /* --gpu_columns N: columns in flight (0 = device default) */
   uint64_t seed;        /* --gpu_seed S: seed of the GPU visiting order */
-  int32_t resync_every; /* --gpu_resync K: FP64 resync of e every K iterations (cost is FP64 every iteration) */
+  int32_t resync_every; /* --gpu_resync K: FP64 resync of e every K iterations (default 10);
+                           the other iterations take the cost of the running e, in FP64 sums */
   int32_t quiet;        /* --quiet: no stdout chatter */
   int32_t n_unknown;    /* unrecognised options seen (reported, not fatal, like the reference) */
 } xt_engine_opts;

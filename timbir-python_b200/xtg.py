@@ -20,12 +20,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(HERE, "lib")
 
-XTG_A_FP32, XTG_A_FP16, XTG_A_TABLE32 = 0, 1, 2
+XTG_A_FP32, XTG_A_FP16, XTG_A_TABLE32, XTG_A_AUTO = 0, 1, 2, 3
 XTG_ORDER_PARALLEL, XTG_ORDER_SEQUENTIAL = 0, 1
 
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
-    "xtg_create", "xtg_destroy", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
+    "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
     "xtg_get_hr", "xtg_set_options", "xtg_upload_sino", "xtg_upload_counts", "xtg_upload_object",
     "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
     "xtg_get_offset", "xtg_set_offset", "xtg_get_magmap", "xtg_set_magmap", "xtg_get_variance",
@@ -245,10 +245,10 @@ class Context:
         h = C.c_void_p()
         _check(lib.xtg_create(C.byref(self._cp), _p(t), _p(a), len(t), C.byref(h)), "xtg_create")
         self.h = h
-        d = np.zeros(10, np.int32)
+        d = np.zeros(11, np.int32)
         lib.xtg_dims(h, _p(d))
         (self.N_x, self.N_y, self.N_z, self.N_time, self.N_r, self.N_t, self.N_p,
-         self.nzb, self.zovl, self.amax) = (int(v) for v in d)
+         self.nzb, self.zovl, self.amax, self.n_masked) = (int(v) for v in d)
 
     def close(self):
         if getattr(self, "h", None):
@@ -283,6 +283,14 @@ class Context:
         out = np.zeros((self.N_p, 65), np.float32)
         _check(self.lib.xtg_get_hr(self.h, _p(out)), "xtg_get_hr")
         return out
+
+    def set_zslab(self, slices):
+        _check(self.lib.xtg_set_zslab(self.h, int(slices)), "xtg_set_zslab")
+
+    def zslab(self):
+        v = C.c_int32()
+        _check(self.lib.xtg_get_zslab(self.h, C.byref(v)), "xtg_get_zslab")
+        return v.value
 
     def set_options(self, a_mode=XTG_A_FP32, order=XTG_ORDER_PARALLEL, max_columns=0, seed=0x5EED5EED):
         _check(self.lib.xtg_set_options(self.h, a_mode, order, max_columns, seed), "xtg_set_options")
@@ -415,10 +423,10 @@ class Context:
         return int(self.lib.xtg_launch_count(self.h))
 
     def last_kernel_time(self):
-        ms, items, rows = C.c_float(), C.c_int64(), C.c_int64()
-        _check(self.lib.xtg_last_kernel_time(self.h, C.byref(ms), C.byref(items), C.byref(rows)),
+        ms, items, launches = C.c_float(), C.c_int64(), C.c_int64()
+        _check(self.lib.xtg_last_kernel_time(self.h, C.byref(ms), C.byref(items), C.byref(launches)),
                "xtg_last_kernel_time")
-        return ms.value, items.value
+        return ms.value, items.value, launches.value
 
 
 # ------------------------------------------------------------ generator ----
