@@ -151,6 +151,40 @@ def upsample_case():
     return out
 
 
+def config_c1():
+    """The reference's CPU-runnable configuration: 4 slices of 128^2, 128 bins,
+    180 views at i degrees, 10 ellipsoids, 2e4 photons/ray, no zinger
+    correction, no NHICD.  The FP64 reference runs 150 iterations (its cost
+    per iteration; the last is the converged cost C*), the FP32 reference the
+    20 iterations the configuration names."""
+    p = common.params(N=128, NT=4, NP=180, nhicd=False)
+    with tempfile.TemporaryDirectory() as d:
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            t, a = common.views(p)
+            xtg.write_view_file("view_info.txt", t, a)
+            x, ax, y, w = common.data(p, t, a, seed=1, n_ell=10, I0=2e4)
+            out = dict(times=t, angles=a, y_sum=np.float64(y.astype(np.float64).sum()),
+                       w_sum=np.float64(w.astype(np.float64).sum()))
+            for double, iters, key in ((True, 150, "costs64"), (False, 20, "costs32")):
+                r = Reference(p, double=double)
+                r.set_sino(y, w)
+                r.init_error_sino()
+                r.srandom2(761521)
+                cs = [r.cost()[0]]
+                for it in range(1, iters + 1):
+                    r.iterate(it)
+                    cs.append(r.cost()[0])
+                out[key] = np.array(cs)
+                if double:
+                    out["x_star"] = r.object().astype(np.float32)
+                r.close()
+        finally:
+            os.chdir(cwd)
+    return out
+
+
 def main():
     if not ref_available():
         sys.exit("oracle/_ref is not built (make -C oracle needs the reference tree)")
@@ -162,8 +196,12 @@ def main():
     np.savez_compressed(os.path.join(HERE, "rng_kat.npz"), table=rng_kat())
     np.savez_compressed(os.path.join(HERE, "nhicd_select.npz"), **nhicd_case())
     np.savez_compressed(os.path.join(HERE, "upsample.npz"), **upsample_case())
+    np.savez_compressed(os.path.join(HERE, "config_c1.npz"), **config_c1())
     print("done")
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["config_c1"]:
+        np.savez_compressed(os.path.join(HERE, "config_c1.npz"), **config_c1())
+    else:
+        main()

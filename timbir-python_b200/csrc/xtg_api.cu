@@ -87,6 +87,7 @@ struct xtg_ctx {
   int zslab_req = 0;  // z slices per ICD work piece; 0 = from the L2 size
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
+  std::vector<cudaEvent_t> tev;  // start/stop pairs of the ICD launches of one iteration
   int have_sino = 0;
   long long launches = 0;
   float last_kms = 0.f;
@@ -538,6 +539,7 @@ void xtg_destroy(xtg_ctx *c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ek0) cudaEventDestroy(c->ek0);
+  for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   if (c->ek1) cudaEventDestroy(c->ek1);
   if (c->st) cudaStreamDestroy(c->st);
   xt_views_free(&c->v);
@@ -1320,6 +1322,15 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
   float kms_total = 0.f;
   long long items_total = 0;
   double vox_mag = 0;
+  // ICD launches are timed with event pairs read once at the end of the
+  // iteration, so the host never waits between launches
+  const size_t npair = (size_t)3 * K;
+  while (c->tev.size() < 2 * npair) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    c->tev.push_back(e);
+  }
+  size_t ntimed = 0;
   for (int j = 0; j < K; j++) {
     const int lo = j * chunk, hi = (j == K - 1) ? n : (j + 1) * chunk;
     if (j == K - 1) {  // the reference's vox_mag covers the last chunk only (XT_ICD_update.c:798)
@@ -1329,20 +1340,17 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
       rc = reset_stats(c);
       if (rc) return rc;
     }
-    CK(cudaEventRecord(c->ek0, c->st));
+    CK(cudaEventRecord(c->tev[2 * ntimed], c->st));
     int rc = run_columns(c, iter, c->d_items, lo, hi - lo, nullptr, 0, 0, 1, 0, -1);
     if (rc) return rc;
-    CK(cudaEventRecord(c->ek1, c->st));
+    CK(cudaEventRecord(c->tev[2 * ntimed + 1], c->st));
+    ntimed++;
     if (j == K - 1) {
       rc = read_stats(c, st, &vox_mag);
       if (rc) return rc;
       rc = reset_stats(c);
       if (rc) return rc;
     }
-    CK(cudaEventSynchronize(c->ek1));
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, c->ek0, c->ek1));
-    kms_total += ms;
     items_total += hi - lo;
     if (c->prm.updateProjOffset > 1) {
       rc = xtg_update_offset(c);
@@ -1352,14 +1360,11 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
     if (rc) return rc;
     if (iter > 1 && !c->prm.no_NHICD) {
       for (int h = 0; h < 2; h++) {
-        CK(cudaEventRecord(c->ek0, c->st));
+        CK(cudaEventRecord(c->tev[2 * ntimed], c->st));
         rc = run_columns(c, iter, c->d_nh, h ? cap0 : 0, 0, c->d_nhcnt + h, 1, key + 17 * (j * 2 + h + 1), 0, 1, -1);
         if (rc) return rc;
-        CK(cudaEventRecord(c->ek1, c->st));
-        CK(cudaEventSynchronize(c->ek1));
-        float ms2 = 0;
-        CK(cudaEventElapsedTime(&ms2, c->ek0, c->ek1));
-        kms_total += ms2;
+        CK(cudaEventRecord(c->tev[2 * ntimed + 1], c->st));
+        ntimed++;
         if (c->prm.updateProjOffset > 1) {
           rc = xtg_update_offset(c);
           if (rc) return rc;
@@ -1367,8 +1372,12 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
       }
     }
   }
-  int hc[2];
-  CK(cudaMemcpyAsync(hc, c->d_nhcnt, 8, cudaMemcpyDeviceToHost, c->st));
+  if (ntimed) CK(cudaEventSynchronize(c->tev[2 * ntimed - 1]));
+  for (size_t i = 0; i < ntimed; i++) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->tev[2 * i], c->tev[2 * i + 1]));
+    kms_total += ms;
+  }
   double tmp;
   int rc = read_stats(c, st, &tmp);
   if (rc) return rc;

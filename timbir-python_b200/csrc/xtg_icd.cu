@@ -21,6 +21,12 @@
 
 namespace xtg {
 
+// Footprint entries a thread loads before it uses any of them (table modes,
+// 16-byte rows): more loads in flight per warp to cover L2/HBM latency.
+#ifndef XTG_UNROLL
+#define XTG_UNROLL 2
+#endif
+
 // surrogate coefficient with fast intrinsics: the step size only needs a few
 // digits, the fixed point of the iteration is unchanged
 __device__ __forceinline__ float qcoef_fast(float d, float sq, float sqp, float c, float p) {
@@ -74,6 +80,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
   float *sNb = sTh + 2 * rowsmax;                         // [9][zmax+2]
   float *sTn = sNb + 9 * (zmax + 2);                      // [2][zmax]
   float *sDelta = sTn + 2 * zmax;                         // [zmax]
+
   __shared__ int sItem;
   __shared__ double sAbs[XTG_THREADS / 32];
   __shared__ unsigned sUpd, sZero;
@@ -189,21 +196,8 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     const int trow0 = t0 + tl * VEC;
     const float *eb = A.e + trow0;
     const float *wb = A.w + trow0;
-    auto accumulate = [&](int off, float a) {
+    auto accumulate_arr = [&](const float (&ev)[VEC], const float (&wv)[VEC], float a) {
       const float a2 = a * a, na = -a;
-      float ev[VEC], wv[VEC];
-      if (VEC == 4) {
-        const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(eb + off));
-        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wb + off));
-        ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
-        wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
-      } else {
-#pragma unroll
-        for (int c = 0; c < VEC; c++) {
-          ev[c] = __ldcg(eb + off + c);
-          wv[c] = __ldg(wb + off + c);
-        }
-      }
       float ew[VEC], q[VEC];
       float qm = 0.f;
 #pragma unroll
@@ -232,6 +226,32 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
         }
       }
     };
+    auto accumulate_vals = [&](const float4 e4, const float4 w4, float a) {
+      float ev[VEC], wv[VEC];
+      const float ea[4] = {e4.x, e4.y, e4.z, e4.w}, wa[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+      for (int c = 0; c < VEC; c++) {
+        ev[c] = ea[c < 4 ? c : 0];
+        wv[c] = wa[c < 4 ? c : 0];
+      }
+      accumulate_arr(ev, wv, a);
+    };
+    auto accumulate = [&](int off, float a) {
+      float ev[VEC], wv[VEC];
+      if (VEC == 4) {
+        const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(eb + off));
+        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wb + off));
+        ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
+        wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
+      } else {
+#pragma unroll
+        for (int c = 0; c < VEC; c++) {
+          ev[c] = __ldcg(eb + off + c);
+          wv[c] = __ldg(wb + off + c);
+        }
+      }
+      accumulate_arr(ev, wv, a);
+    };
     if (tl < tln && !skip_all) {
       if (AMODE == 0) {
         for (int v = vg; v < V; v += vgs) {
@@ -240,6 +260,25 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
 #pragma unroll
           for (int s = 0; s < AS; s++)
             if (s < n) accumulate(off + s * G.N_t, sVal[s * vmax + v]);
+        }
+      } else if (VEC == 4) {
+        int e = vg;
+        for (; e + (XTG_UNROLL - 1) * vgs < ne; e += XTG_UNROLL * vgs) {
+          int2 en[XTG_UNROLL];
+          float4 e4[XTG_UNROLL], w4[XTG_UNROLL];
+#pragma unroll
+          for (int u = 0; u < XTG_UNROLL; u++) en[u] = sEnt[e + u * vgs];
+#pragma unroll
+          for (int u = 0; u < XTG_UNROLL; u++) {
+            e4[u] = __ldcg(reinterpret_cast<const float4 *>(eb + en[u].x));
+            w4[u] = __ldg(reinterpret_cast<const float4 *>(wb + en[u].x));
+          }
+#pragma unroll
+          for (int u = 0; u < XTG_UNROLL; u++) accumulate_vals(e4[u], w4[u], __int_as_float(en[u].y));
+        }
+        for (; e < ne; e += vgs) {
+          const int2 en = sEnt[e];
+          accumulate(en.x, __int_as_float(en.y));
         }
       } else {
         for (int e = vg; e < ne; e += vgs) {
@@ -465,12 +504,12 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
   }
 }
 
-size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode) {
+size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec) {
   size_t b = 0;
   if (amode == 0)
     b += (size_t)vmax * (4 * 2 + 4 * (size_t)as);  // sPack, sView, sVal
   else
-    b += (size_t)vmax * 8;                         // sEnt (vmax = longest column run)
+    b += (size_t)vmax * 8;                         // sEnt
   b += 2 * 8 * 128 * 4;                            // sRed
   b += 2 * (size_t)zmax * zovl * 4;                // sTh
   b += 9 * (size_t)(zmax + 2) * 4;                 // sNb
@@ -478,6 +517,7 @@ size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode) {
   b += (size_t)zmax * 4;                           // sDelta
   return b;
 }
+
 
 typedef void (*IcdKernel)(DevGeo, IcdArgs, int, int);
 
@@ -520,7 +560,7 @@ cudaError_t launch_magmap_zero(const DevGeo &G, const IcdArgs &A, int grid, cuda
 
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st) {
-  const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as, amode);
+  const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as, amode, vec);
   IcdKernel k = icd_kernel(vec, amode, seq, as);
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -534,7 +574,7 @@ cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, in
 }
 
 int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl) {
-  const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as, amode);
+  const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as, amode, vec);
   IcdKernel k = icd_kernel(vec, amode, seq, as);
   int nb = 0;
   cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

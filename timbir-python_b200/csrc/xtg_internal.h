@@ -65,7 +65,7 @@ cudaError_t launch_fp(const DevGeo &G, const FpArgs &F, int mode, int ns, cudaSt
 cudaError_t launch_table_count(const DevGeo &G, const TableArgs &T, int ns, long long *count, cudaStream_t st);
 cudaError_t launch_table_fill(const DevGeo &G, const TableArgs &T, int ns, cudaStream_t st);
 
-size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode);
+size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec);
 cudaError_t launch_magmap_zero(const DevGeo &G, const IcdArgs &A, int grid, cudaStream_t st);
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st);
