@@ -346,7 +346,8 @@ def run_ours(args):
                      "alg_bytes_per_launch": alg_per_launch, "ms_per_launch": ms_per_launch,
                      "icd_launches_timed": n_icd, "bytes_per_voxel_update": b_upd, "nnz_per_column": nnz,
                      "dram_bytes_per_voxel_update": dpu,
-                     "traffic_note": "ncu dram bytes per voxel update of a random-pass launch x voxel updates per launch",
+                     "traffic_note": "ncu DRAM bytes per voxel (iteration average of a random-pass and an NHICD "
+                                     "launch, 384^2 capture, cold L2) x voxel updates per launch",
                      "kernel_ms_per_step": kms / args.steps, "column_items_per_step": rows / args.steps},
         "gpu_launches": launches,
         "clocks": clocks,
