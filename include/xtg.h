@@ -139,6 +139,13 @@ int xtg_amatrix(xtg_ctx *ctx, int32_t n, const int32_t *rows, const int32_t *col
 int xtg_forward_project(xtg_ctx *ctx, float *ax);
 /* e = y - A x - d in FP32 (initErrorSinogam, XT_ICD_update.c:538-597). */
 int xtg_init_error_sino(xtg_ctx *ctx);
+/* Warm start: object := filtered backprojection of y - d (ramp filter and
+ * linearly interpolated backprojection over each frame's views; 0 outside
+ * the reconstruction disk, clamped at 0 with positivity), then
+ * e = y - Ax - d.  No XT_Engine counterpart: the reference starts from zero
+ * or a coarser stage (initObject, XT_ICD_update.c:443-536), and its
+ * launchers compute FBP outside the engine (XT_FBP_Reconstruction.py). */
+int xtg_init_object_fbp(xtg_ctx *ctx);
 /* e = y - A x - d with FP64 accumulation, rounded to FP32: the periodic
  * resync that removes the drift of incremental FP32 updates.  The same pass
  * yields the MAP cost of the current object in FP64 (outputs may be NULL). */

@@ -245,3 +245,42 @@ def test_zslab_pieces_update_each_voxel_once(zslab):
         z1 = c.N_z if b == c.nzb - 1 else (b + 1) * zstep
         want = float(np.abs(dx[0, b * zstep:z1, 7, 9]).sum())
         assert m[0, b, 7, 9] == pytest.approx(want, rel=1e-5, abs=1e-12)
+
+
+@pytest.mark.parametrize("name", ["plain3d", "coarse_xy2", "timbir4d", "offset_zero_mean"])
+def test_fbp_start_matches_checker(name):
+    """xtg_init_object_fbp against the FP64 numpy restatement (FP32 sums on
+    the device: 1e-4 of the image's maximum), then e = y - Ax - d exactly."""
+    import fbp_check
+    c, g, p = ctx_for(name)
+    c.upload_sino(g["y"], g["w"])
+    c.init_fbp()
+    want = fbp_check.fbp(p, g["times"], g["angles"], g["y"])
+    got = c.object()
+    assert got.shape == want.shape
+    assert np.max(np.abs(got - want)) <= 1e-4 * np.abs(want).max()
+    e_fbp = c.error_sino()
+    c.upload_object(got)
+    c.init_error_sino()
+    assert np.array_equal(c.error_sino(), e_fbp)
+
+
+def test_fbp_start_lowers_cost_of_early_iterations():
+    """Config-1 geometry (128^2 x 4, 180 views): after 3 iterations from the
+    FBP start the MAP cost is below that of 3 iterations from zero."""
+    p = common.params(N=128, NT=4, NP=180, nhicd=False)
+    t, a = common.views(p)
+    x, ax, y, w = common.data(p, t, a, seed=1, n_ell=10, I0=2e4)
+    costs = {}
+    for start in ("zero", "fbp"):
+        c = xtg.Context(p, t, a)
+        c.upload_sino(y, w)
+        if start == "fbp":
+            c.init_fbp()
+        else:
+            c.init_error_sino()
+        for it in range(1, 4):
+            c.iteration(it)
+        costs[start] = c.resync_fp64()[0]
+        c.close()
+    assert costs["fbp"] < costs["zero"], costs

@@ -66,6 +66,9 @@ cudaError_t launch_table_count(const DevGeo &G, const TableArgs &T, int ns, long
 cudaError_t launch_table_fill(const DevGeo &G, const TableArgs &T, int ns, cudaStream_t st);
 
 size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec);
+cudaError_t launch_fbp(const DevGeo &G, const float *y, const float *d, float *q, const float *cosv,
+                       const float *sinv, const int *view_idx, const int *view_start, const int *view_num,
+                       const int *col_rank, float *x, cudaStream_t st);
 cudaError_t launch_magmap_zero(const DevGeo &G, const IcdArgs &A, int grid, cudaStream_t st);
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st);

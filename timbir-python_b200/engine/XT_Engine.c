@@ -357,8 +357,13 @@ int main(int argc, char **argv) {
     }
   }
 
-  /* e = y - A x - d, then the cost before ICD (XT_ICD_update.c:998-1007) */
-  if ((rc = xtg_init_error_sino(ctx))) {
+  /* e = y - A x - d, then the cost before ICD (XT_ICD_update.c:998-1007);
+   * --gpu_fbp_start replaces the zero start by the FBP image */
+  if (P.initICD == 0 && O.fbp_start)
+    rc = xtg_init_object_fbp(ctx);
+  else
+    rc = xtg_init_error_sino(ctx);
+  if (rc) {
     logf_("ERROR: %s\n", xtg_last_error());
     return 1;
   }

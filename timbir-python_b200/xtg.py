@@ -25,7 +25,7 @@ XTG_ORDER_PARALLEL, XTG_ORDER_SEQUENTIAL = 0, 1
 
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
-    "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
+    "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_init_object_fbp", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
     "xtg_get_hr", "xtg_set_options", "xtg_upload_sino", "xtg_upload_counts", "xtg_upload_object",
     "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
     "xtg_get_offset", "xtg_set_offset", "xtg_get_magmap", "xtg_set_magmap", "xtg_get_variance",
@@ -283,6 +283,9 @@ class Context:
         out = np.zeros((self.N_p, 65), np.float32)
         _check(self.lib.xtg_get_hr(self.h, _p(out)), "xtg_get_hr")
         return out
+
+    def init_fbp(self):
+        _check(self.lib.xtg_init_object_fbp(self.h), "xtg_init_object_fbp")
 
     def set_zslab(self, slices):
         _check(self.lib.xtg_set_zslab(self.h, int(slices)), "xtg_set_zslab")
