@@ -21,15 +21,17 @@ PKG = os.path.join(ROOT, "timbir-python_b200")
 def declared(header):
     txt = open(os.path.join(ROOT, "include", header)).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(xtg(?:en)?_[a-z0-9_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b((?:xtg(?:en)?|xtc)_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_headers_match_binding_lists():
     assert declared("xtg.h") == sorted(xtg.XTG_SYMBOLS)
     assert declared("xt_gen.h") == sorted(xtg.XTGEN_SYMBOLS)
+    assert declared("xtg_cnn.h") == sorted(xtg.XTC_SYMBOLS)
 
 
-@pytest.mark.parametrize("lib,names", [("libxtgpu.so", "XTG_SYMBOLS"), ("libxtgen.so", "XTGEN_SYMBOLS")])
+@pytest.mark.parametrize("lib,names", [("libxtgpu.so", "XTG_SYMBOLS"), ("libxtgen.so", "XTGEN_SYMBOLS"),
+                                       ("libxtgpu.so", "XTC_SYMBOLS")])
 def test_libraries_export_declared_symbols(lib, names):
     L = C.CDLL(os.path.join(PKG, "lib", lib))
     for s in getattr(xtg, names):

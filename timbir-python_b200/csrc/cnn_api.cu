@@ -1,0 +1,78 @@
+// cnn_api.cu -- C ABI of the warm-start network (include/xtg_cnn.h).
+#include <cstdio>
+
+#include "../../include/xtg.h"
+#include "../../include/xtg_cnn.h"
+#include "xtg_cnn_internal.h"
+
+void xtg_set_error_text(const char *msg);  // xtg_api.cu
+
+namespace {
+int *g_err = nullptr;  // device flag: a bounded wait in a tensor-core kernel gave up
+
+int fail(cudaError_t e, const char *what) {
+  char b[256];
+  snprintf(b, sizeof b, "%s: %s", what, cudaGetErrorString(e));
+  xtg_set_error_text(b);
+  return XTG_E_CUDA;
+}
+
+int check_err_flag(const char *what) {
+  int h = 0;
+  cudaError_t e = cudaMemcpy(&h, g_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(e, what);
+  if (h) {
+    cudaMemset(g_err, 0, sizeof(int));
+    char b[256];
+    snprintf(b, sizeof b, "%s: tensor-core pipeline wait timed out", what);
+    xtg_set_error_text(b);
+    return XTG_E_TIMEOUT;
+  }
+  return 0;
+}
+
+int ensure_err() {
+  if (g_err) return 0;
+  cudaError_t e = cudaMalloc(&g_err, sizeof(int));
+  if (e != cudaSuccess) return fail(e, "xtc: error flag");
+  e = cudaMemset(g_err, 0, sizeof(int));
+  return e == cudaSuccess ? 0 : fail(e, "xtc: error flag");
+}
+}  // namespace
+
+extern "C" {
+
+int xtc_conv3d(const void *in, const void *w, const float *bias, void *out, int32_t nb, int32_t Y, int32_t X,
+               int32_t Z, int32_t cin, int32_t cout, int32_t kpad, int32_t epi, int32_t sign) {
+  if (!in || !w || !out || (epi == 0 && !bias) || epi < 0 || epi > 2 || (sign != 1 && sign != -1)) {
+    xtg_set_error_text("xtc_conv3d: bad argument");
+    return XTG_E_ARG;
+  }
+  int rc = ensure_err();
+  if (rc) return rc;
+  xtc::ConvShape s{nb, Y, X, Z, cin, cout, kpad};
+  cudaError_t e = xtc::conv_forward(s, (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)w, bias, out, epi, sign,
+                                    g_err, 0);
+  if (e != cudaSuccess) return fail(e, "xtc_conv3d");
+  e = cudaStreamSynchronize(0);
+  if (e != cudaSuccess) return fail(e, "xtc_conv3d");
+  return check_err_flag("xtc_conv3d");
+}
+
+int xtc_conv3d_wgrad(const void *in, const void *dout, float *dw, int32_t nb, int32_t Y, int32_t X, int32_t Z,
+                     int32_t cin, int32_t cout) {
+  if (!in || !dout || !dw) {
+    xtg_set_error_text("xtc_conv3d_wgrad: bad argument");
+    return XTG_E_ARG;
+  }
+  int rc = ensure_err();
+  if (rc) return rc;
+  xtc::ConvShape s{nb, Y, X, Z, cin, cout, 0};
+  cudaError_t e = xtc::conv_wgrad(s, (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)dout, dw, g_err, 0);
+  if (e != cudaSuccess) return fail(e, "xtc_conv3d_wgrad");
+  e = cudaStreamSynchronize(0);
+  if (e != cudaSuccess) return fail(e, "xtc_conv3d_wgrad");
+  return check_err_flag("xtc_conv3d_wgrad");
+}
+
+}  // extern "C"

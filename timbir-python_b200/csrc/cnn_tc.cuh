@@ -1,0 +1,117 @@
+// cnn_tc.cuh -- Blackwell tensor-core (tcgen05 / TMEM) building blocks for
+// the warm-start network's implicit-GEMM convolutions.
+//
+// One CTA of 128 threads computes a 128 x N tile of D = A B^T (BF16 inputs,
+// FP32 accumulator in tensor memory).  Operand tiles are staged in shared
+// memory by the CTA's threads in the canonical no-swizzle ("interleaved")
+// layouts the MMA descriptors describe, 64 K elements per stage, two stages:
+// the threads gather stage s+1 while the tensor core works on stage s.  One
+// elected thread issues tcgen05.mma and commits each stage to an mbarrier.
+//
+// Shared-memory operand layouts (element = 2 bytes, T = 8 elements = 16 B):
+//   K-major  (row r of the M or N dimension, K index k):
+//       byte (k/8) * (ROWS*16) + r*16 + (k%8)*2
+//       descriptor: leading byte offset (between the two 8-element K halves of
+//       one MMA) = ROWS*16, stride byte offset (between 8-row groups) = 128.
+//   MN-major (row r, K index k):
+//       byte (k/8) * (ROWS*16) + (r/8)*128 + (k%8)*16 + (r%8)*2
+//       descriptor: leading byte offset (between 8-element K groups) = ROWS*16,
+//       stride byte offset (between 8-row groups) = 128.
+// In both, one MMA (K = 16) spans two 8-element K groups, so the descriptor
+// start address advances by 2*ROWS*16 bytes per MMA along K.
+// Descriptor bit layout and instruction-descriptor fields follow the sm100
+// UMMA definitions (CUTLASS cute/arch/mma_sm100_desc.hpp).
+#pragma once
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace xtc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, no swizzle, sm100 version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// instruction descriptor: BF16 x BF16 -> F32, M = 128, N, majors (0 = K, 1 = MN)
+__host__ __device__ constexpr uint32_t idesc_bf16(int n, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// bounded wait for the mbarrier phase with the given parity; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, long long limit = 1ll << 26) {
+  const uint32_t a = smem_u32(mbar);
+  for (long long i = 0; i < limit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// TMEM allocation by one full warp; the base address lands in *dst (shared)
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t base, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(ncols) : "memory");
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// TMEM columns to allocate for N accumulator columns (power of two, >= 32)
+__host__ __device__ constexpr uint32_t tmem_cols(int n) {
+  return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : 256u;
+}
+
+}  // namespace xtc

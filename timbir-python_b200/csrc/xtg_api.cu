@@ -37,6 +37,9 @@ static void set_err(const char *fmt, ...) {
   va_end(ap);
 }
 
+// error text from the warm-start network's entry points (cnn_api.cu)
+void xtg_set_error_text(const char *msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+
 #define CK(call)                                                                             \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \

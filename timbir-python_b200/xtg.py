@@ -35,6 +35,8 @@ XTG_SYMBOLS = [
     "xtg_update_variance", "xtg_device_bytes", "xtg_launch_count", "xtg_last_kernel_time",
     "xtg_nhicd_threshold_noalloc",
 ]
+# warm-start network entry points (include/xtg_cnn.h), also in libxtgpu.so
+XTC_SYMBOLS = ["xtc_conv3d", "xtc_conv3d_wgrad"]
 XTGEN_SYMBOLS = [
     "xtgen_views_uniform", "xtgen_views_interlaced", "xtgen_write_view_file", "xtgen_phantom",
     "xtgen_forward", "xtgen_measure", "xtgen_write_bin", "xtgen_geometry", "xtgen_amatrix",
