@@ -32,6 +32,42 @@ int xtc_conv3d(const void *in, const void *w, const float *bias, void *out, int3
 int xtc_conv3d_wgrad(const void *in, const void *dout, float *dw, int32_t nb, int32_t Y, int32_t X, int32_t Z,
                      int32_t cin, int32_t cout);
 
+/* ---- the warm-start network ------------------------------------------------
+ * A 3D encoder-decoder over channels-last volumes: four levels with 32, 48,
+ * 64 and 96 channels, two 3x3x3 convolutions + ReLU per level on each side,
+ * 2x average pooling down, nearest 2x upsampling + skip concatenation up and
+ * a 1x1 head.  Input: the FBP image and the image after a few ICD equits
+ * (FP32 [nb][Y][X][Z] each, the engine's device layout with nb = frames);
+ * output: icd + correction.  Y, X, Z must be multiples of 8.  About 1.44 M
+ * FP32 master parameters; BF16 weights and activations, FP32 accumulation. */
+typedef struct xtc_net xtc_net;
+
+/* He-initialised weights from the seed; the head starts at zero, so the new
+ * network returns its ICD input unchanged. */
+int xtc_net_create(uint64_t seed, xtc_net **net);
+void xtc_net_destroy(xtc_net *net);
+int64_t xtc_net_param_count(const xtc_net *net);
+/* which = 0: parameters, 1: gradients of the last xtc_net_backward (host copy) */
+int xtc_net_get_params(const xtc_net *net, float *host, int32_t which);
+int xtc_net_set_params(xtc_net *net, const float *host);
+int xtc_net_save(const xtc_net *net, const char *path);
+int xtc_net_load(xtc_net *net, const char *path);
+/* out = network(fbp, icd) on device buffers */
+int xtc_net_forward(xtc_net *net, const float *fbp, const float *icd, float *out, int32_t nb, int32_t Y, int32_t X,
+                    int32_t Z);
+/* forward and backward of loss = mean(((out - target) * 100)^2); gradients
+ * replace the previous ones; *loss (host) receives the loss */
+int xtc_net_backward(xtc_net *net, const float *fbp, const float *icd, const float *target, int32_t nb, int32_t Y,
+                     int32_t X, int32_t Z, double *loss);
+/* one Adam step (beta 0.9 / 0.999, eps 1e-8) with the current gradients */
+int xtc_net_adam_step(xtc_net *net, float lr);
+/* `steps` Adam steps on random py x px x pz patches (batch of them per step)
+ * cut from nvol device volume triples (fbp[i], icd[i], target[i], each
+ * [Y][X][Z]); losses[step] (host, optional) receives each step's loss. */
+int xtc_net_train(xtc_net *net, const float *const *fbp, const float *const *icd, const float *const *target,
+                  int32_t nvol, int32_t Y, int32_t X, int32_t Z, int32_t py, int32_t px, int32_t pz, int32_t batch,
+                  int32_t steps, float lr, uint64_t seed, float *losses);
+
 #ifdef __cplusplus
 }
 #endif

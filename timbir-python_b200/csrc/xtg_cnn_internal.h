@@ -18,4 +18,24 @@ cudaError_t conv_forward(const ConvShape &s, const __nv_bfloat16 *in, const __nv
 cudaError_t conv_wgrad(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, float *dw, int *err,
                        cudaStream_t st);
 
+void pack_input(long long nv, const float *a, const float *b, float scale, __nv_bfloat16 *out, cudaStream_t st);
+void avgpool(int nb, int Y, int X, int Z, int C, const __nv_bfloat16 *in, __nv_bfloat16 *out, cudaStream_t st);
+void avgpool_back(int nb, int Y, int X, int Z, int C, const float *dout, float *din, cudaStream_t st);
+void up_concat(int nb, int Y, int X, int Z, int Ca, int Cb, const __nv_bfloat16 *a, const __nv_bfloat16 *skip,
+               __nv_bfloat16 *out, cudaStream_t st);
+void up_concat_back(int nb, int Y, int X, int Z, int Ca, int Cb, const float *dout, float *da, float *dskip,
+                    cudaStream_t st);
+void relu_back(long long nv, int C, const float *dpost, const __nv_bfloat16 *post, __nv_bfloat16 *dpre, float *dbias,
+               cudaStream_t st);
+void to_f32(long long n, const __nv_bfloat16 *a, float *b, cudaStream_t st);
+void head(long long nv, int C, const __nv_bfloat16 *h, const float *w, const float *bias, const float *base, float scale,
+          float *y, const float *target, double *loss, float *dh32, float *dw, float *db, cudaStream_t st);
+void pack_weights(int cin_real, int cin, int cout, int kpad, int kpad_t, const float *P, __nv_bfloat16 *W,
+                  __nv_bfloat16 *Wt, cudaStream_t st);
+void fold_wgrad(int cin_real, int cin, int cout, const float *g, float *out, cudaStream_t st);
+void adam(long long n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2, float eps, int t,
+          cudaStream_t st);
+void crop(int np, const float *const *src, const int4 *org, int Y, int X, int Z, int py, int px, int pz, float *dst,
+          cudaStream_t st);
+
 }  // namespace xtc

@@ -36,7 +36,9 @@ XTG_SYMBOLS = [
     "xtg_nhicd_threshold_noalloc",
 ]
 # warm-start network entry points (include/xtg_cnn.h), also in libxtgpu.so
-XTC_SYMBOLS = ["xtc_conv3d", "xtc_conv3d_wgrad"]
+XTC_SYMBOLS = ["xtc_conv3d", "xtc_conv3d_wgrad", "xtc_net_create", "xtc_net_destroy", "xtc_net_param_count",
+               "xtc_net_get_params", "xtc_net_set_params", "xtc_net_save", "xtc_net_load", "xtc_net_forward",
+               "xtc_net_backward", "xtc_net_adam_step", "xtc_net_train"]
 XTGEN_SYMBOLS = [
     "xtgen_views_uniform", "xtgen_views_interlaced", "xtgen_write_view_file", "xtgen_phantom",
     "xtgen_forward", "xtgen_measure", "xtgen_write_bin", "xtgen_geometry", "xtgen_amatrix",
@@ -432,6 +434,81 @@ class Context:
         _check(self.lib.xtg_last_kernel_time(self.h, C.byref(ms), C.byref(items), C.byref(launches)),
                "xtg_last_kernel_time")
         return ms.value, items.value, launches.value
+
+
+# ------------------------------------------------------ warm-start network --
+class WarmNet:
+    """The learned warm start (include/xtg_cnn.h) over device buffers.  Volume
+    arguments are CUDA tensors (torch) or raw device addresses (int)."""
+
+    def __init__(self, seed=1):
+        lib = gpu_lib()
+        self.lib = lib
+        lib.xtc_net_create.argtypes = [C.c_uint64, C.POINTER(C.c_void_p)]
+        lib.xtc_net_destroy.argtypes = [C.c_void_p]
+        lib.xtc_net_destroy.restype = None
+        lib.xtc_net_param_count.argtypes = [C.c_void_p]
+        lib.xtc_net_param_count.restype = C.c_int64
+        lib.xtc_net_adam_step.argtypes = [C.c_void_p, C.c_float]
+        lib.xtc_net_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                      C.c_uint64, C.c_void_p]
+        h = C.c_void_p()
+        _check(lib.xtc_net_create(C.c_uint64(seed), C.byref(h)), "xtc_net_create")
+        self.h = h
+        self.n_params = int(lib.xtc_net_param_count(h))
+
+    @staticmethod
+    def _dev(t):
+        return C.c_void_p(t if isinstance(t, int) else t.data_ptr())
+
+    def params(self, which=0):
+        out = np.zeros(self.n_params, np.float32)
+        _check(self.lib.xtc_net_get_params(self.h, _p(out), int(which)), "xtc_net_get_params")
+        return out
+
+    def set_params(self, p):
+        p = _f32(p)
+        assert p.size == self.n_params
+        _check(self.lib.xtc_net_set_params(self.h, _p(p)), "xtc_net_set_params")
+
+    def forward(self, fbp, icd, out, shape):
+        nb, Y, X, Z = shape
+        _check(self.lib.xtc_net_forward(self.h, self._dev(fbp), self._dev(icd), self._dev(out), nb, Y, X, Z),
+               "xtc_net_forward")
+
+    def backward(self, fbp, icd, target, shape):
+        nb, Y, X, Z = shape
+        loss = C.c_double()
+        _check(self.lib.xtc_net_backward(self.h, self._dev(fbp), self._dev(icd), self._dev(target), nb, Y, X, Z,
+                                         C.byref(loss)), "xtc_net_backward")
+        return loss.value
+
+    def adam_step(self, lr):
+        _check(self.lib.xtc_net_adam_step(self.h, C.c_float(lr)), "xtc_net_adam_step")
+
+    def train(self, fbp, icd, target, vol_shape, patch, batch, steps, lr=1e-3, seed=7):
+        """fbp / icd / target: lists of device volumes [Y][X][Z]; returns the losses."""
+        n = len(fbp)
+        arr = C.c_void_p * n
+        pf, pi, pt = (arr(*[self._dev(t) for t in lst]) for lst in (fbp, icd, target))
+        losses = np.zeros(steps, np.float32)
+        Y, X, Z = vol_shape
+        py, px, pz = patch
+        _check(self.lib.xtc_net_train(self.h, pf, pi, pt, n, Y, X, Z, py, px, pz, batch, steps, C.c_float(lr),
+                                      C.c_uint64(seed), _p(losses)), "xtc_net_train")
+        return losses
+
+    def save(self, path):
+        _check(self.lib.xtc_net_save(self.h, str(path).encode()), "xtc_net_save")
+
+    def load(self, path):
+        _check(self.lib.xtc_net_load(self.h, str(path).encode()), "xtc_net_load")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.xtc_net_destroy(self.h)
+            self.h = None
 
 
 # ------------------------------------------------------------ generator ----
