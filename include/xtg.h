@@ -146,6 +146,13 @@ int xtg_init_error_sino(xtg_ctx *ctx);
  * or a coarser stage (initObject, XT_ICD_update.c:443-536), and its
  * launchers compute FBP outside the engine (XT_FBP_Reconstruction.py). */
 int xtg_init_object_fbp(xtg_ctx *ctx);
+/* Device-to-device object transfer in the engine's device layout
+ * [N_time][N_y][N_x][N_z] (z fastest; the channels-last volume layout of
+ * xtg_cnn.h with nb = N_time).  xtg_object_from_device zeroes columns outside
+ * the reconstruction disk and clamps at 0 with positivity; e is not updated
+ * (call xtg_init_error_sino).  No reference counterpart. */
+int xtg_object_to_device(xtg_ctx *ctx, float *dst);
+int xtg_object_from_device(xtg_ctx *ctx, const float *src);
 /* e = y - A x - d with FP64 accumulation, rounded to FP32: the periodic
  * resync that removes the drift of incremental FP32 updates.  The same pass
  * yields the MAP cost of the current object in FP64 (outputs may be NULL). */

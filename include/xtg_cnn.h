@@ -68,6 +68,17 @@ int xtc_net_train(xtc_net *net, const float *const *fbp, const float *const *icd
                   int32_t nvol, int32_t Y, int32_t X, int32_t Z, int32_t py, int32_t px, int32_t pz, int32_t batch,
                   int32_t steps, float lr, uint64_t seed, float *losses);
 
+/* ---- learned warm start on an engine context (xtg.h) ----------------------
+ * object := FBP (xtg_init_object_fbp), then `equits` ICD iterations numbered
+ * 1..equits, then the network's estimate from (FBP, current image).  The
+ * estimate is kept (*used = 1) only if its MAP cost is below that of the ICD
+ * image (both with e = y - Ax - d recomputed); otherwise the ICD image stays
+ * (*used = 0) -- the fallback.  ICD continues with iteration equits + 1.
+ * Needs N_x, N_y, N_z multiples of 8. */
+struct xtg_ctx;
+int xtg_init_object_learned(struct xtg_ctx *ctx, xtc_net *net, int32_t equits, int32_t *used, double *cost_net,
+                            double *cost_icd);
+
 #ifdef __cplusplus
 }
 #endif

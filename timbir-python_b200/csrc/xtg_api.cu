@@ -806,6 +806,35 @@ int xtg_upload_object(xtg_ctx *c, const float *x) {
   return 0;
 }
 
+// object from a device buffer in the engine's device layout, 0 outside the
+// reconstruction disk and clamped at 0 with positivity
+__global__ void k_obj_from_dev(DevGeo G, const int *rank, const float *src, float *dst) {
+  const long long n = (long long)G.N_time * G.N_y * G.N_x * G.N_z;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long col = i / G.N_z;
+    const int jk = (int)(col % ((long long)G.N_y * G.N_x));
+    float v = rank[jk] >= 0 ? src[i] : 0.f;
+    if (G.positivity && !(v > 0.f)) v = 0.f;  // also maps NaN to 0
+    dst[i] = v;
+  }
+}
+
+int xtg_object_to_device(xtg_ctx *c, float *dst) {
+  if (!c || !dst) return XTG_E_ARG;
+  CK(cudaMemcpyAsync(dst, c->d_x, c->nvox * 4, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int xtg_object_from_device(xtg_ctx *c, const float *src) {
+  if (!c || !src) return XTG_E_ARG;
+  k_obj_from_dev<<<std::min<unsigned>(blocks_for(c->nvox, 256), 8192), 256, 0, c->st>>>(c->G, c->d_rank, src, c->d_x);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
 int xtg_download_object(xtg_ctx *c, float *x) {
   if (!c || !x) return XTG_E_ARG;
   if (!c->d_tmp && dalloc(c, &c->d_tmp, c->nvox)) return XTG_E_CUDA;

@@ -1,0 +1,53 @@
+// xtg_warm.cu -- the learned warm start on an engine context: FBP, a few ICD
+// equits, then the network's estimate, kept only if it lowers the MAP cost.
+#include <cstdio>
+
+#include "../../include/xtg.h"
+#include "../../include/xtg_cnn.h"
+
+void xtg_set_error_text(const char *msg);
+
+extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t equits, int32_t *used, double *cost_net,
+                                       double *cost_icd) {
+  if (!ctx || !net || equits < 0) return XTG_E_ARG;
+  int32_t d[11];
+  int rc = xtg_dims(ctx, d);
+  if (rc) return rc;
+  const int N_x = d[0], N_y = d[1], N_z = d[2], N_time = d[3];
+  if (N_x % 8 || N_y % 8 || N_z % 8) {
+    xtg_set_error_text("xtg_init_object_learned: N_x, N_y and N_z must be multiples of 8");
+    return XTG_E_ARG;
+  }
+  const size_t nvox = (size_t)N_time * N_y * N_x * N_z;
+  float *buf = nullptr;
+  cudaError_t e = cudaMalloc(&buf, 3 * nvox * sizeof(float));
+  if (e != cudaSuccess) {
+    char b[200];
+    snprintf(b, sizeof b, "xtg_init_object_learned: %s", cudaGetErrorString(e));
+    xtg_set_error_text(b);
+    return XTG_E_CUDA;
+  }
+  float *fbp = buf, *icd = buf + nvox, *out = buf + 2 * nvox;
+  double ci = 0, cn = 0;
+  int use = 0;
+  do {
+    if ((rc = xtg_init_object_fbp(ctx)) || (rc = xtg_object_to_device(ctx, fbp))) break;
+    for (int it = 1; it <= equits && !rc; it++) rc = xtg_icd_iteration(ctx, it, nullptr);
+    // both candidates are costed from a freshly computed e = y - Ax - d
+    if (rc || (rc = xtg_object_to_device(ctx, icd)) || (rc = xtg_init_error_sino(ctx)) ||
+        (rc = xtg_map_cost_running(ctx, &ci, nullptr, nullptr)))
+      break;
+    if ((rc = xtc_net_forward(net, fbp, icd, out, N_time, N_y, N_x, N_z))) break;
+    if ((rc = xtg_object_from_device(ctx, out)) || (rc = xtg_init_error_sino(ctx)) ||
+        (rc = xtg_map_cost_running(ctx, &cn, nullptr, nullptr)))
+      break;
+    use = cn < ci;
+    if (!use && ((rc = xtg_object_from_device(ctx, icd)) || (rc = xtg_init_error_sino(ctx)))) break;
+  } while (0);
+  cudaFree(buf);
+  if (rc) return rc;
+  if (used) *used = use;
+  if (cost_net) *cost_net = cn;
+  if (cost_icd) *cost_icd = ci;
+  return 0;
+}

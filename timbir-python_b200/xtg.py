@@ -25,7 +25,8 @@ XTG_ORDER_PARALLEL, XTG_ORDER_SEQUENTIAL = 0, 1
 
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
-    "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_init_object_fbp", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
+    "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_init_object_fbp", "xtg_object_to_device",
+    "xtg_object_from_device", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
     "xtg_get_hr", "xtg_set_options", "xtg_upload_sino", "xtg_upload_counts", "xtg_upload_object",
     "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
     "xtg_get_offset", "xtg_set_offset", "xtg_get_magmap", "xtg_set_magmap", "xtg_get_variance",
@@ -38,7 +39,7 @@ XTG_SYMBOLS = [
 # warm-start network entry points (include/xtg_cnn.h), also in libxtgpu.so
 XTC_SYMBOLS = ["xtc_conv3d", "xtc_conv3d_wgrad", "xtc_net_create", "xtc_net_destroy", "xtc_net_param_count",
                "xtc_net_get_params", "xtc_net_set_params", "xtc_net_save", "xtc_net_load", "xtc_net_forward",
-               "xtc_net_backward", "xtc_net_adam_step", "xtc_net_train"]
+               "xtc_net_backward", "xtc_net_adam_step", "xtc_net_train", "xtg_init_object_learned"]
 XTGEN_SYMBOLS = [
     "xtgen_views_uniform", "xtgen_views_interlaced", "xtgen_write_view_file", "xtgen_phantom",
     "xtgen_forward", "xtgen_measure", "xtgen_write_bin", "xtgen_geometry", "xtgen_amatrix",
@@ -290,6 +291,20 @@ class Context:
 
     def init_fbp(self):
         _check(self.lib.xtg_init_object_fbp(self.h), "xtg_init_object_fbp")
+
+    def object_to_device(self, dst):
+        _check(self.lib.xtg_object_to_device(self.h, WarmNet._dev(dst)), "xtg_object_to_device")
+
+    def object_from_device(self, src):
+        _check(self.lib.xtg_object_from_device(self.h, WarmNet._dev(src)), "xtg_object_from_device")
+
+    def init_learned(self, net, equits=2):
+        """Learned warm start; returns (used, cost_net, cost_icd).  Continue ICD
+        with iteration equits + 1."""
+        used, cn, ci = C.c_int32(), C.c_double(), C.c_double()
+        _check(self.lib.xtg_init_object_learned(self.h, net.h, int(equits), C.byref(used), C.byref(cn), C.byref(ci)),
+               "xtg_init_object_learned")
+        return bool(used.value), cn.value, ci.value
 
     def set_zslab(self, slices):
         _check(self.lib.xtg_set_zslab(self.h, int(slices)), "xtg_set_zslab")
