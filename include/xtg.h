@@ -153,6 +153,21 @@ int xtg_init_object_fbp(xtg_ctx *ctx);
  * (call xtg_init_error_sino).  No reference counterpart. */
 int xtg_object_to_device(xtg_ctx *ctx, float *dst);
 int xtg_object_from_device(xtg_ctx *ctx, const float *src);
+
+/* upsample_object_bilinear_2D / _3D (XT_ICD_update.c:354-436) on the GPU:
+ * in [nt][nz][ny][nx] (host) -> out [nt][2nz or nz][2ny][2nx] (host), bit for
+ * bit the reference's values (the initICD 2 / 3 starts of XT_Engine). */
+int xtg_upsample(xtg_ctx *ctx, const float *in, float *out, int32_t nt, int32_t nz, int32_t ny, int32_t nx,
+                 int32_t with_z);
+
+/* Multi-resolution start, the launcher's coarse-to-fine stages in one call:
+ * reconstruct the same data on a grid with voxels twice as large in x-y (and
+ * z with with_z), from its FBP image, for coarse_iters ICD iterations; then
+ * object := that reconstruction upsampled as above (0 outside the disk,
+ * clamped with positivity) and e = y - Ax - d.  The coarse context is kept
+ * for later calls.  No XT_Engine counterpart (the launcher runs the stages
+ * as separate XT_Engine processes with --initICD 2/3). */
+int xtg_init_object_multires(xtg_ctx *ctx, int32_t coarse_iters, int32_t with_z);
 /* e = y - A x - d with FP64 accumulation, rounded to FP32: the periodic
  * resync that removes the drift of incremental FP32 updates.  The same pass
  * yields the MAP cost of the current object in FP64 (outputs may be NULL). */

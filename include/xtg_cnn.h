@@ -36,9 +36,9 @@ int xtc_conv3d_wgrad(const void *in, const void *dout, float *dw, int32_t nb, in
  * A 3D encoder-decoder over channels-last volumes: four levels with 32, 48,
  * 64 and 96 channels, two 3x3x3 convolutions + ReLU per level on each side,
  * 2x average pooling down, nearest 2x upsampling + skip concatenation up and
- * a 1x1 head.  Input: the FBP image and the image after a few ICD equits
- * (FP32 [nb][Y][X][Z] each, the engine's device layout with nb = frames);
- * output: icd + correction.  Y, X, Z must be multiples of 8.  About 1.44 M
+ * a 1x1 head.  Input: the FBP image and a start image (FP32 [nb][Y][X][Z]
+ * each, the engine's device layout with nb = frames); output: start image +
+ * correction (the `icd` argument below is the start image).  Y, X, Z must be multiples of 8.  About 1.44 M
  * FP32 master parameters; BF16 weights and activations, FP32 accumulation. */
 typedef struct xtc_net xtc_net;
 
@@ -69,15 +69,16 @@ int xtc_net_train(xtc_net *net, const float *const *fbp, const float *const *icd
                   int32_t steps, float lr, uint64_t seed, float *losses);
 
 /* ---- learned warm start on an engine context (xtg.h) ----------------------
- * object := FBP (xtg_init_object_fbp), then `equits` ICD iterations numbered
- * 1..equits, then the network's estimate from (FBP, current image).  The
- * estimate is kept (*used = 1) only if its MAP cost is below that of the ICD
- * image (both with e = y - Ax - d recomputed); otherwise the ICD image stays
- * (*used = 0) -- the fallback.  ICD continues with iteration equits + 1.
+ * The network's inputs are the FBP image (xtg_init_object_fbp) and the
+ * multi-resolution start (xtg_init_object_multires with coarse_iters coarse
+ * iterations, z halved too when N_z is even and >= 16); its estimate is kept
+ * (*used = 1) only if its MAP cost is below the multi-resolution start's
+ * (both with e = y - Ax - d recomputed); otherwise the multi-resolution start
+ * stays (*used = 0) -- the fallback.  ICD then continues at iteration 1.
  * Needs N_x, N_y, N_z multiples of 8. */
 struct xtg_ctx;
-int xtg_init_object_learned(struct xtg_ctx *ctx, xtc_net *net, int32_t equits, int32_t *used, double *cost_net,
-                            double *cost_icd);
+int xtg_init_object_learned(struct xtg_ctx *ctx, xtc_net *net, int32_t coarse_iters, int32_t *used,
+                            double *cost_net, double *cost_base);
 
 #ifdef __cplusplus
 }

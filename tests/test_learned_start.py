@@ -1,12 +1,17 @@
-"""The learned warm start end to end on the engine (small geometry: 64^2 x 16
-voxels, 128 views, 1e4 photons/ray, 0.5 % zingers):
+"""The multi-resolution and learned warm starts end to end on the engine
+(small geometry: 64^2 x 16 voxels, 128 views, 1e4 photons/ray, 0.5 %
+zingers):
 
-  * an untrained network (zero head) returns its ICD input, which is not
-    lower in cost, so the fallback keeps the ICD image;
+  * the GPU upsampling reproduces the reference's upsample_object_bilinear_2D
+    and _3D bit for bit (tests/golden/upsample.npz);
+  * the multi-resolution start reaches (1 + 1e-3) of the converged cost in
+    fewer fine iterations than the FBP start;
+  * an untrained network (zero head) returns its start image, which is not
+    lower in cost, so the fallback keeps the multi-resolution start;
   * a network trained on 16 phantoms reconstructed by the engine lowers the
-    MAP cost of a held-out phantom's start below the ICD image it was given,
-    and the reconstruction from it reaches (1 + 1e-3) of the converged cost in
-    fewer iterations than the FBP start.
+    MAP cost of a held-out phantom's start below the multi-resolution start
+    it was given, and needs no more iterations than it to reach
+    (1 + 1e-3) of the converged cost.
 """
 import os
 import sys
@@ -46,36 +51,56 @@ def iters_to(c, start_iter, target, limit=200):
     return None
 
 
-def test_untrained_network_falls_back_to_icd_image():
+def converged(seed=77):
+    c = held_out_ctx(seed)
+    c.init_fbp()
+    for it in range(1, 121):
+        c.iteration(it)
+    return c.resync_fp64()[0]
+
+
+def test_upsampling_bit_exact():
+    g = dict(np.load(os.path.join(common.GOLDEN, "upsample.npz")))
+    c = held_out_ctx()
+    assert np.array_equal(c.upsample(g["inp"][None], with_z=False)[0], g["xy"])
+    assert np.array_equal(c.upsample(g["inp"][None], with_z=True)[0], g["xyz"])
+
+
+def test_multires_start_beats_fbp_start():
+    target = converged() * (1 + 1e-3)
+    c = held_out_ctx()
+    c.init_multires(20)
+    n_multi = iters_to(c, 1, target)
+    c = held_out_ctx()
+    c.init_fbp()
+    n_fbp = iters_to(c, 1, target)
+    print("iterations to 1e-3: multires", n_multi, "fbp", n_fbp)
+    assert n_multi is not None and n_fbp is not None and n_multi < n_fbp
+
+
+def test_untrained_network_falls_back_to_multires_start():
     c = held_out_ctx()
     net = xtg.WarmNet(seed=2)
-    used, cn, ci = c.init_learned(net, 2)
-    # the zero head returns the ICD image itself: equal cost, so it is not used
-    assert not used and cn == ci
-    # the context holds the ICD image with a fresh e: its cost is the one reported
+    used, cn, ci = c.init_learned(net, 20)
+    # the zero head returns the start image itself: equal cost, so it is not used
+    assert not used and cn == pytest.approx(ci, rel=1e-12)
+    # the context holds the multi-resolution start with a fresh e
     assert c.cost_running()[0] == pytest.approx(ci, rel=1e-12)
     net.close()
 
 
-def test_trained_network_lowers_start_cost_and_iterations():
-    data, shape = tw.make_set(16, N, NT, NP, equits=2, target_iters=40, seed=500, log=lambda *a: None)
+def test_trained_network_lowers_start_cost():
+    data, shape = tw.make_set(16, N, NT, NP, coarse_iters=20, target_iters=40, seed=500, log=lambda *a: None)
     net, losses = tw.train(data, shape, steps=400, batch=8, patch=(32, 32, 16), log=lambda *a: None)
     assert losses[-50:].mean() < losses[:50].mean()
-    # converged cost of the held-out phantom
+    target = converged() * (1 + 1e-3)
     c = held_out_ctx()
-    c.init_fbp()
-    for it in range(1, 121):
-        c.iteration(it)
-    c_star = c.resync_fp64()[0]
-    target = c_star * (1 + 1e-3)
-    c = held_out_ctx()
-    used, cn, ci = c.init_learned(net, 2)
+    used, cn, ci = c.init_learned(net, 20)
     assert used and cn < ci, (cn, ci)
-    n_learned = iters_to(c, 3, target)
+    n_learned = iters_to(c, 1, target)
     c = held_out_ctx()
-    c.init_fbp()
-    n_fbp = iters_to(c, 1, target)
-    print("iterations to 1e-3:", "learned", n_learned, "+2", "fbp", n_fbp)
-    assert n_learned is not None and n_fbp is not None
-    assert n_learned + 2 <= n_fbp
+    c.init_multires(20)
+    n_multi = iters_to(c, 1, target)
+    print("iterations to 1e-3: learned", n_learned, "multires", n_multi, "start costs", cn, ci)
+    assert n_learned is not None and n_multi is not None and n_learned <= n_multi
     net.close()

@@ -87,6 +87,8 @@ struct xtg_ctx {
   unsigned long long seed = 0x5eed5eedULL;
   int sm_count = 0;
   long long l2_bytes = 0;
+  std::vector<double> t_in, a_in;  // view times / angles as given (for the coarse context)
+  xtg_ctx *coarse = nullptr;      // multi-resolution start: the 2x coarser grid
   int zslab_req = 0;  // z slices per ICD work piece; 0 = from the L2 size
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
@@ -532,6 +534,7 @@ int xtg_abi_version(void) { return XTG_ABI_VERSION; }
 
 void xtg_destroy(xtg_ctx *c) {
   if (!c) return;
+  if (c->coarse) xtg_destroy(c->coarse);
   void *ptrs[] = {c->d_y, c->d_w, c->d_e, c->d_d, c->d_x, c->d_mag, c->d_hr, c->d_cos, c->d_sin, c->d_ax,
                   c->d_filt, c->d_tmp, c->d_num, c->d_den, c->d_thr, c->d_var, c->d_view_idx, c->d_view_start,
                   c->d_view_num, c->d_fov, c->d_mcols, c->d_rank, c->d_counter, c->d_nhcnt, c->d_err, c->d_kth,
@@ -571,6 +574,8 @@ int xtg_create(const xt_params *prm, const double *times, const double *angles, 
   }
   xtg_ctx *c = new xtg_ctx();
   c->prm = *prm;
+  c->t_in.assign(times, times + n);
+  c->a_in.assign(angles, angles + n);
   char err[512];
   if (xt_geom_derive(prm, &c->g, err, sizeof(err)) != 0) {
     set_err("%s", err);
@@ -833,6 +838,145 @@ int xtg_object_from_device(xtg_ctx *c, const float *src) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
   return 0;
+}
+
+// One axis of upsample_object_bilinear_2D/3D (XT_ICD_update.c:354-436): a
+// line of n values becomes 2n,
+//   out[0] = in[0], out[1] = (3 in[0] + in[1]) / 4,
+//   out[2k] = (in[k-1] + 3 in[k]) / 4, out[2k+1] = (3 in[k] + in[k+1]) / 4,
+//   out[2n-2] = (in[n-2] + 3 in[n-1]) / 4, out[2n-1] = in[n-1],
+// in double and rounded to float once; the reference's y pass writes the
+// interior odd rows as (3*b + b') in float first (`3*buffer` is an int times
+// a float), reproduced with f32_odd.  Lines are (outer, axis, inner) strided.
+__global__ void k_up1d(long long outer, int n, long long inner, const float *in, float *out, int f32_odd) {
+  const long long tot = outer * 2 * n * inner;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+    const long long r = i % inner;
+    const long long q = i / inner;
+    const int o = (int)(q % (2 * n));
+    const long long b = (q / (2 * n)) * n * inner + r;
+    auto at = [&](int k) { return in[b + (long long)k * inner]; };
+    float v;
+    if (n == 1) {
+      v = at(0);
+    } else if (o == 0) {
+      v = at(0);
+    } else if (o == 2 * n - 1) {
+      v = at(n - 1);
+    } else if (o == 1) {
+      v = (float)__dmul_rn(__dadd_rn(__dmul_rn(3.0, (double)at(0)), (double)at(1)), 0.25);
+    } else if (o == 2 * n - 2) {
+      v = (float)__dmul_rn(__dadd_rn((double)at(n - 2), __dmul_rn(3.0, (double)at(n - 1))), 0.25);
+    } else if ((o & 1) == 0) {
+      const int k = o / 2;
+      v = (float)__dmul_rn(__dadd_rn((double)at(k - 1), __dmul_rn(3.0, (double)at(k))), 0.25);
+    } else {
+      const int k = o / 2;
+      if (f32_odd)
+        v = (float)__dmul_rn((double)__fadd_rn(__fmul_rn(3.0f, at(k)), at(k + 1)), 0.25);
+      else
+        v = (float)__dmul_rn(__dadd_rn(__dmul_rn(3.0, (double)at(k)), (double)at(k + 1)), 0.25);
+    }
+    out[i] = v;
+  }
+}
+
+// 2x upsampling of [nt][nz][ny][nx] volumes (in the layout given by the
+// strides below) through two scratch buffers: x, then y, then (with_z) z
+static int upsample_dev(xtg_ctx *c, const float *in, float *out, int nt, int nz, int ny, int nx, int with_z,
+                        bool zfast) {
+  const size_t n1 = (size_t)nt * nz * ny * 2 * nx, n2 = n1 * 2;
+  float *b1 = nullptr, *b2 = nullptr;
+  CK(cudaMalloc(&b1, n1 * 4));
+  if (cudaMalloc(&b2, n2 * 4) != cudaSuccess) {
+    cudaFree(b1);
+    set_err("upsample: out of device memory");
+    return XTG_E_CUDA;
+  }
+  const unsigned g = (unsigned)std::min<size_t>(blocks_for(n2 * 2, 256), (size_t)c->sm_count * 16);
+  if (zfast) {  // [t][y][x][z]
+    k_up1d<<<g, 256, 0, c->st>>>((long long)nt * ny, nx, nz, in, b1, 0);
+    k_up1d<<<g, 256, 0, c->st>>>(nt, ny, (long long)2 * nx * nz, b1, with_z ? b2 : out, 1);
+    if (with_z) k_up1d<<<g, 256, 0, c->st>>>((long long)nt * 2 * ny * 2 * nx, nz, 1, b2, out, 0);
+  } else {  // [t][z][y][x]
+    k_up1d<<<g, 256, 0, c->st>>>((long long)nt * nz * ny, nx, 1, in, b1, 0);
+    k_up1d<<<g, 256, 0, c->st>>>((long long)nt * nz, ny, 2 * nx, b1, with_z ? b2 : out, 1);
+    if (with_z) k_up1d<<<g, 256, 0, c->st>>>(nt, nz, (long long)4 * ny * nx, b2, out, 0);
+  }
+  c->launches += with_z ? 3 : 2;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  cudaFree(b1);
+  cudaFree(b2);
+  if (e != cudaSuccess) {
+    set_err("upsample: %s", cudaGetErrorString(e));
+    return XTG_E_CUDA;
+  }
+  return 0;
+}
+
+int xtg_upsample(xtg_ctx *c, const float *in, float *out, int32_t nt, int32_t nz, int32_t ny, int32_t nx,
+                 int32_t with_z) {
+  if (!c || !in || !out || nt < 1 || nz < 1 || ny < 1 || nx < 1) return XTG_E_ARG;
+  const size_t nin = (size_t)nt * nz * ny * nx, nout = nin * (with_z ? 8 : 4);
+  float *din = nullptr, *dout = nullptr;
+  CK(cudaMalloc(&din, nin * 4));
+  if (cudaMalloc(&dout, nout * 4) != cudaSuccess) {
+    cudaFree(din);
+    set_err("xtg_upsample: out of device memory");
+    return XTG_E_CUDA;
+  }
+  int rc = 0;
+  if (cudaMemcpy(din, in, nin * 4, cudaMemcpyHostToDevice) != cudaSuccess) rc = XTG_E_CUDA;
+  if (!rc) rc = upsample_dev(c, din, dout, nt, nz, ny, nx, with_z, false);
+  if (!rc && cudaMemcpy(out, dout, nout * 4, cudaMemcpyDeviceToHost) != cudaSuccess) rc = XTG_E_CUDA;
+  cudaFree(din);
+  cudaFree(dout);
+  return rc;
+}
+
+int xtg_init_object_multires(xtg_ctx *c, int32_t coarse_iters, int32_t with_z) {
+  if (!c || coarse_iters < 0) return XTG_E_ARG;
+  if (!c->have_sino) {
+    set_err("xtg_init_object_multires: no sinogram uploaded");
+    return XTG_E_STATE;
+  }
+  const xt_geom &g = c->g;
+  if (g.N_x % 2 || g.N_y % 2 || (with_z && g.N_z % 2)) {
+    set_err("xtg_init_object_multires: grid not divisible by 2");
+    return XTG_E_ARG;
+  }
+  if (c->coarse && (c->coarse->g.N_z == g.N_z) != !with_z) {
+    xtg_destroy(c->coarse);
+    c->coarse = nullptr;
+  }
+  if (!c->coarse) {
+    // the same scan with voxels twice as large (the launcher's coarser stage)
+    xt_params cp = c->prm;
+    cp.delta_xy *= 2;
+    if (with_z) cp.delta_z *= 2;
+    int rc = xtg_create(&cp, c->t_in.data(), c->a_in.data(), (int32_t)c->t_in.size(), &c->coarse);
+    if (rc) return rc;
+    if ((rc = xtg_set_options(c->coarse, c->a_mode, XTG_ORDER_PARALLEL, c->max_columns, c->seed))) return rc;
+  }
+  xtg_ctx *cc = c->coarse;
+  // the same measurement, weights (already scaled by the variance) and offset
+  CK(cudaMemcpyAsync(cc->d_y, c->d_y, c->ns * 4, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(cc->d_w, c->d_w, c->ns * 4, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(cc->d_d, c->d_d, c->nrt * 4, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(cc->d_var, c->d_var, 4, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  cc->have_sino = 1;
+  int rc = xtg_init_object_fbp(cc);
+  for (int it = 1; it <= coarse_iters && !rc; it++) rc = xtg_icd_iteration(cc, it, nullptr);
+  if (rc) return rc;
+  const xt_geom &h = cc->g;
+  if (!c->d_tmp && dalloc(c, &c->d_tmp, c->nvox)) return XTG_E_CUDA;
+  rc = upsample_dev(c, cc->d_x, c->d_tmp, h.N_time, h.N_z, h.N_y, h.N_x, with_z, true);
+  if (rc) return rc;
+  rc = xtg_object_from_device(c, c->d_tmp);
+  if (rc) return rc;
+  return xtg_init_error_sino(c);
 }
 
 int xtg_download_object(xtg_ctx *c, float *x) {

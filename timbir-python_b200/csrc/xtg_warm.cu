@@ -1,5 +1,6 @@
-// xtg_warm.cu -- the learned warm start on an engine context: FBP, a few ICD
-// equits, then the network's estimate, kept only if it lowers the MAP cost.
+// xtg_warm.cu -- the learned warm start on an engine context: the FBP image
+// and the multi-resolution start go through the network, whose estimate is
+// kept only if it lowers the MAP cost.
 #include <cstdio>
 
 #include "../../include/xtg.h"
@@ -7,9 +8,9 @@
 
 void xtg_set_error_text(const char *msg);
 
-extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t equits, int32_t *used, double *cost_net,
-                                       double *cost_icd) {
-  if (!ctx || !net || equits < 0) return XTG_E_ARG;
+extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coarse_iters, int32_t *used,
+                                       double *cost_net, double *cost_base) {
+  if (!ctx || !net || coarse_iters < 0) return XTG_E_ARG;
   int32_t d[11];
   int rc = xtg_dims(ctx, d);
   if (rc) return rc;
@@ -32,10 +33,10 @@ extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t equit
   int use = 0;
   do {
     if ((rc = xtg_init_object_fbp(ctx)) || (rc = xtg_object_to_device(ctx, fbp))) break;
-    for (int it = 1; it <= equits && !rc; it++) rc = xtg_icd_iteration(ctx, it, nullptr);
-    // both candidates are costed from a freshly computed e = y - Ax - d
-    if (rc || (rc = xtg_object_to_device(ctx, icd)) || (rc = xtg_init_error_sino(ctx)) ||
-        (rc = xtg_map_cost_running(ctx, &ci, nullptr, nullptr)))
+    // the multi-resolution start (it ends with e = y - Ax - d recomputed, so
+    // both candidates are costed from a fresh e)
+    if ((rc = xtg_init_object_multires(ctx, coarse_iters, N_z % 2 == 0 && N_z >= 16)) ||
+        (rc = xtg_object_to_device(ctx, icd)) || (rc = xtg_map_cost_running(ctx, &ci, nullptr, nullptr)))
       break;
     if ((rc = xtc_net_forward(net, fbp, icd, out, N_time, N_y, N_x, N_z))) break;
     if ((rc = xtg_object_from_device(ctx, out)) || (rc = xtg_init_error_sino(ctx)) ||
@@ -48,6 +49,6 @@ extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t equit
   if (rc) return rc;
   if (used) *used = use;
   if (cost_net) *cost_net = cn;
-  if (cost_icd) *cost_icd = ci;
+  if (cost_base) *cost_base = ci;
   return 0;
 }

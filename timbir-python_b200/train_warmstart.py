@@ -7,9 +7,10 @@ Training set: seeded ellipsoid phantoms of N^2 x NT voxels (default 256^2 x
 32, 512 views uniform over 180 degrees, 1e4 photons/ray, 0.5 % zingers with
 the generalized-Huber correction on, NHICD on -- the plain-3D-at-scale
 statistics at half the size and half the views).  For each phantom the GPU
-engine forms the network's inputs, the FBP image and the image after
-`equits` ICD iterations from it, and the target, the reconstruction after
-`target_iters` iterations.  Training: Adam (lr 1e-3), batches of random
+engine forms the network's inputs, the FBP image and the multi-resolution
+start (`coarse_iters` ICD iterations on the 2x coarser grid, upsampled), and
+the target, the reconstruction after `target_iters` further iterations on
+the fine grid.  Training: Adam (lr 1e-3), batches of random
 64 x 64 x 32 patches.  Data generation and training run on the GPU through
 the library; the host only draws the Poisson counts and sequences calls.
 """
@@ -36,9 +37,10 @@ def params(N, NT, NP, zinger=True):
         num_threads=1, positivity=1, no_NHICD=0)
 
 
-def make_set(n_vol, N=256, NT=32, NP=512, n_ell=30, I0=1e4, zfrac=0.005, equits=2, target_iters=40, seed=1000,
-             log=print):
-    """(fbp, icd, target) device tensors [N][N][NT] per phantom, and the geometry."""
+def make_set(n_vol, N=256, NT=32, NP=512, n_ell=30, I0=1e4, zfrac=0.005, coarse_iters=30, target_iters=40,
+             seed=1000, log=print):
+    """(fbp, multi-resolution start, target) device tensors [N][N][NT] per
+    phantom, and the geometry."""
     import torch
     p = params(N, NT, NP)
     t, a = xtg.round_views(*xtg.views_uniform(NP))
@@ -56,11 +58,10 @@ def make_set(n_vol, N=256, NT=32, NP=512, n_ell=30, I0=1e4, zfrac=0.005, equits=
         ctx.init_fbp()
         f = torch.empty(shape, device="cuda")
         ctx.object_to_device(f)
-        for it in range(1, equits + 1):
-            ctx.iteration(it)
+        ctx.init_multires(coarse_iters, with_z=NT % 2 == 0 and NT >= 16)
         q = torch.empty(shape, device="cuda")
         ctx.object_to_device(q)
-        for it in range(equits + 1, target_iters + 1):
+        for it in range(1, target_iters + 1):
             ctx.iteration(it)
         g = torch.empty(shape, device="cuda")
         ctx.object_to_device(g)
@@ -90,17 +91,17 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--nt", type=int, default=32)
     ap.add_argument("--views", type=int, default=512)
-    ap.add_argument("--equits", type=int, default=2)
+    ap.add_argument("--coarse-iters", type=int, default=30)
     ap.add_argument("--target-iters", type=int, default=40)
     args = ap.parse_args()
     t0 = time.time()
-    data, shape = make_set(args.volumes, args.n, args.nt, args.views, equits=args.equits,
+    data, shape = make_set(args.volumes, args.n, args.nt, args.views, coarse_iters=args.coarse_iters,
                            target_iters=args.target_iters)
     t1 = time.time()
     net, losses = train(data, shape, steps=args.steps, batch=args.batch)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     net.save(args.out)
-    info = {"volumes": args.volumes, "shape": shape, "views": args.views, "equits": args.equits,
+    info = {"volumes": args.volumes, "shape": shape, "views": args.views, "coarse_iters": args.coarse_iters,
             "target_iters": args.target_iters, "steps": args.steps, "batch": args.batch,
             "data_s": t1 - t0, "train_s": time.time() - t1, "loss_first50": float(losses[:50].mean()),
             "loss_last50": float(losses[-50:].mean()), "params": net.n_params}

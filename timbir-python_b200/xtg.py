@@ -26,7 +26,7 @@ XTG_ORDER_PARALLEL, XTG_ORDER_SEQUENTIAL = 0, 1
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
     "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_init_object_fbp", "xtg_object_to_device",
-    "xtg_object_from_device", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
+    "xtg_object_from_device", "xtg_upsample", "xtg_init_object_multires", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
     "xtg_get_hr", "xtg_set_options", "xtg_upload_sino", "xtg_upload_counts", "xtg_upload_object",
     "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
     "xtg_get_offset", "xtg_set_offset", "xtg_get_magmap", "xtg_set_magmap", "xtg_get_variance",
@@ -292,18 +292,28 @@ class Context:
     def init_fbp(self):
         _check(self.lib.xtg_init_object_fbp(self.h), "xtg_init_object_fbp")
 
+    def upsample(self, a, with_z=True):
+        a = _f32(a)
+        nt, nz, ny, nx = a.shape
+        out = np.zeros((nt, 2 * nz if with_z else nz, 2 * ny, 2 * nx), np.float32)
+        _check(self.lib.xtg_upsample(self.h, _p(a), _p(out), nt, nz, ny, nx, int(with_z)), "xtg_upsample")
+        return out
+
+    def init_multires(self, coarse_iters=40, with_z=True):
+        _check(self.lib.xtg_init_object_multires(self.h, int(coarse_iters), int(with_z)), "xtg_init_object_multires")
+
     def object_to_device(self, dst):
         _check(self.lib.xtg_object_to_device(self.h, WarmNet._dev(dst)), "xtg_object_to_device")
 
     def object_from_device(self, src):
         _check(self.lib.xtg_object_from_device(self.h, WarmNet._dev(src)), "xtg_object_from_device")
 
-    def init_learned(self, net, equits=2):
-        """Learned warm start; returns (used, cost_net, cost_icd).  Continue ICD
-        with iteration equits + 1."""
+    def init_learned(self, net, coarse_iters=30):
+        """Learned warm start over the multi-resolution start; returns
+        (used, cost_net, cost_base).  ICD continues at iteration 1."""
         used, cn, ci = C.c_int32(), C.c_double(), C.c_double()
-        _check(self.lib.xtg_init_object_learned(self.h, net.h, int(equits), C.byref(used), C.byref(cn), C.byref(ci)),
-               "xtg_init_object_learned")
+        _check(self.lib.xtg_init_object_learned(self.h, net.h, int(coarse_iters), C.byref(used), C.byref(cn),
+                                                C.byref(ci)), "xtg_init_object_learned")
         return bool(used.value), cn.value, ci.value
 
     def set_zslab(self, slices):
