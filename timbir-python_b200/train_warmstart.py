@@ -1,12 +1,15 @@
 """Trains the learned warm start (include/xtg_cnn.h) on phantoms reconstructed
 by this engine, and saves its weights.
 
-    python timbir-python_b200/train_warmstart.py --out timbir-python_b200/weights/warmstart_plain3d.bin
+    python timbir-python_b200/train_warmstart.py --out timbir-python_b200/weights/warmstart_plain3d.bin \
+        --n 512 --nt 64 --views 1024 --volumes 24 --target-iters 30
 
-Training set: seeded ellipsoid phantoms of N^2 x NT voxels (default 256^2 x
-32, 512 views uniform over 180 degrees, 1e4 photons/ray, 0.5 % zingers with
-the generalized-Huber correction on, NHICD on -- the plain-3D-at-scale
-statistics at half the size and half the views).  For each phantom the GPU
+(the committed weights; their .json records the run).  Training set: seeded
+ellipsoid phantoms of N^2 x NT voxels (default 256^2 x 32 with 512 views;
+the committed weights use the plain-3D-at-scale geometry, 512^2 x 64 with
+1024 views), views uniform over 180 degrees, 1e4 photons/ray, 0.5 % zingers
+with the generalized-Huber correction on, NHICD on; phantom seeds 1000 and
+up, distinct from the benchmark's.  For each phantom the GPU
 engine forms the network's inputs, the FBP image and the multi-resolution
 start (`coarse_iters` ICD iterations on the 2x coarser grid, upsampled), and
 the target, the reconstruction after `target_iters` further iterations on
