@@ -168,6 +168,43 @@ def base_config(w, amode):
 WEIGHTS = os.path.join(ROOT, "timbir-python_b200", "weights", "warmstart_plain3d.bin")
 
 
+# (cin, cout, level) of the warm-start network's 3x3x3 convolutions
+NET_LAYERS = [(2, 32, 0), (32, 32, 0), (32, 48, 1), (48, 48, 1), (48, 64, 2), (64, 64, 2), (64, 96, 3), (96, 96, 3),
+              (160, 64, 2), (64, 64, 2), (112, 48, 1), (48, 48, 1), (80, 32, 0), (32, 32, 0)]
+
+
+def network_roofline(ctx, net, coarse_iters, reps=3):
+    """The warm-start network's forward pass over the whole volume (the
+    inference inside the learned start), timed with CUDA events: algorithmic
+    FLOPs (2 x 27 x cin x cout per output voxel and layer) over time, against
+    the measured dense BF16 tensor-core peak."""
+    import torch
+    shape = (ctx.N_time, ctx.N_y, ctx.N_x, ctx.N_z)
+    f, q, o = (torch.empty(shape, device="cuda") for _ in range(3))
+    ctx.init_fbp()
+    ctx.object_to_device(f)
+    ctx.init_multires(coarse_iters)
+    ctx.object_to_device(q)
+    net.forward(f, q, o, shape)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.forward(f, q, o, shape)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    vox = ctx.N_time * ctx.N_y * ctx.N_x * ctx.N_z
+    flops = sum(2.0 * 27 * ci * co * vox / 8 ** lvl for ci, co, lvl in NET_LAYERS)
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+        kind = "measured (MEASURED_PEAKS.json bf16_tflops, burst)"
+    except Exception:
+        peak, kind = 1590.0, "fallback 1.59 PFLOP/s"
+    return {"forward_ms": ms, "tflop": flops / 1e12, "achieved_tflops": flops / ms / 1e9, "peak_tflops": peak,
+            "frac": flops / ms / 1e9 / peak, "peak_kind": kind, "bound": "tensor"}
+
+
 def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, coarse_iters=30):
     """Seconds to MAP cost <= (1 + tol) C* from four starts:
       zero     -- the reference's start, plain ICD with the benchmark's A storage;
@@ -247,6 +284,7 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
         out[kind] = {"s": secs if c <= target else None, "iterations": it, "cost": c,
                      "a_mode": {v: k for k, v in AMODES.items()}[am], **extra}
     if net is not None:
+        out["network"] = network_roofline(ctx, net, coarse_iters)
         net.close()
     ctx.set_options(a_mode=AMODES[amode])
     z = out["zero"].get("s")

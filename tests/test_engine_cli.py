@@ -63,3 +63,15 @@ def test_engine_parallel_schedule_files_and_cost(name, tmp_path):
     c = got["cost_n0.bin"].astype(np.float64)
     assert np.all(np.diff(c) <= 1e-6 * np.abs(c[:-1]))
     assert c[-1] <= float(want["cost_n0.bin"][-1]) * (1 + 1e-2)
+
+
+@pytest.mark.parametrize("start", [["--gpu_fbp_start"], ["--gpu_multires_start", "10"]])
+def test_engine_warm_start_switches(start, tmp_path):
+    """The launcher's command plus a warm-start switch runs end to end: the
+    same output files, and a cost that never increases after the start (what
+    the starts gain is measured by bench.py and tests/test_learned_start.py;
+    on this 36-view toy case the FBP image itself costs more than zero)."""
+    got, want = run_engine("engine_plain", tmp_path, ["--quiet"] + start)
+    c = got["cost_n0.bin"].astype(np.float64)
+    assert np.all(np.isfinite(c)) and c.size == want["cost_n0.bin"].size
+    assert np.all(np.diff(c) <= 1e-6 * np.abs(c[:-1]))

@@ -29,6 +29,7 @@
 
 #include "xt_cli.h"
 #include "xtg.h"
+#include "xtg_cnn.h"
 
 static FILE *g_log = NULL;
 static int g_dbl = 0;
@@ -358,11 +359,26 @@ int main(int argc, char **argv) {
   }
 
   /* e = y - A x - d, then the cost before ICD (XT_ICD_update.c:998-1007);
-   * --gpu_fbp_start replaces the zero start by the FBP image */
-  if (P.initICD == 0 && O.fbp_start)
+   * with initICD 0 the zero start can be replaced by the learned, the
+   * multi-resolution or the FBP start */
+  if (P.initICD == 0 && O.learned[0]) {
+    xtc_net *net = NULL;
+    int32_t used = 0;
+    double cn = 0, cb = 0;
+    rc = xtc_net_create(1, &net);
+    if (!rc) rc = xtc_net_load(net, O.learned);
+    if (!rc) rc = xtg_init_object_learned(ctx, net, O.multires_iters > 0 ? O.multires_iters : 30, &used, &cn, &cb);
+    if (!rc)
+      logf_("XT_Engine: learned start %s (network start cost %f, multi-resolution start cost %f)\n",
+            used ? "used" : "not lower in cost, multi-resolution start kept", cn, cb);
+    xtc_net_destroy(net);
+  } else if (P.initICD == 0 && O.multires_iters > 0) {
+    rc = xtg_init_object_multires(ctx, O.multires_iters, N_z % 2 == 0 && N_z >= 16);
+  } else if (P.initICD == 0 && O.fbp_start) {
     rc = xtg_init_object_fbp(ctx);
-  else
+  } else {
     rc = xtg_init_error_sino(ctx);
+  }
   if (rc) {
     logf_("ERROR: %s\n", xtg_last_error());
     return 1;

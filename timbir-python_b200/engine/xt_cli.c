@@ -10,7 +10,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-enum { OPT_POS = 300, OPT_DOUBLE, OPT_AFP16, OPT_SEQ, OPT_COLS, OPT_SEED, OPT_RESYNC, OPT_QUIET, OPT_HELP, OPT_AMODE, OPT_FBP };
+enum { OPT_POS = 300, OPT_DOUBLE, OPT_AFP16, OPT_SEQ, OPT_COLS, OPT_SEED, OPT_RESYNC, OPT_QUIET, OPT_HELP, OPT_AMODE, OPT_FBP, OPT_MULTIRES, OPT_LEARNED };
 
 int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
   /* option table of XT_Init.c:457-506: names, letters and argument kinds */
@@ -67,6 +67,8 @@ int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
       {"gpu_afp16", no_argument, 0, OPT_AFP16},
       {"gpu_amode", required_argument, 0, OPT_AMODE},
       {"gpu_fbp_start", no_argument, 0, OPT_FBP},
+      {"gpu_multires_start", required_argument, 0, OPT_MULTIRES},
+      {"gpu_learned_start", required_argument, 0, OPT_LEARNED},
       {"gpu_sequential", no_argument, 0, OPT_SEQ},
       {"gpu_columns", required_argument, 0, OPT_COLS},
       {"gpu_seed", required_argument, 0, OPT_SEED},
@@ -144,6 +146,8 @@ int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
         break;
       case OPT_SEQ: o->sequential = 1; break;
       case OPT_FBP: o->fbp_start = 1; break;
+      case OPT_MULTIRES: o->multires_iters = atoi(optarg); break;
+      case OPT_LEARNED: snprintf(o->learned, sizeof o->learned, "%s", optarg); break;
       case OPT_COLS: o->columns = atoi(optarg); break;
       case OPT_SEED: o->seed = strtoull(optarg, NULL, 10); break;
       case OPT_RESYNC: o->resync_every = atoi(optarg); break;
@@ -151,7 +155,7 @@ int xt_cli_parse(int argc, char **argv, xt_params *p, xt_engine_opts *o) {
       case OPT_HELP:
         printf("XT_Engine: TIMBIR/MBIR reconstruction on one B200; options as the reference XT_Engine,\n"
                "plus --positivity 0|1 --real_is_double --gpu_amode fp32|table32|fp16|auto --gpu_afp16\n"
-               "--gpu_fbp_start --gpu_sequential --gpu_columns N\n"
+               "--gpu_fbp_start --gpu_multires_start N --gpu_learned_start WEIGHTS --gpu_sequential --gpu_columns N\n"
                "--gpu_seed S --gpu_resync K --quiet\n");
         return 1;
       default:

@@ -15,6 +15,8 @@
 
 typedef struct {
   int32_t fbp_start;    /* --gpu_fbp_start: with initICD 0, start from the FBP image instead of zero */
+  int32_t multires_iters; /* --gpu_multires_start N: with initICD 0, the multi-resolution start with N coarse iterations */
+  char learned[512];    /* --gpu_learned_start PATH: with initICD 0, the learned start with these weights */
   int32_t a_mode;       /* --gpu_amode fp32|table32|fp16|auto (XTG_A_*); --gpu_afp16 = fp16 */
   int32_t sequential;   /* --gpu_sequential: reference visiting order, one column at a time */
   int32_t columns;      /* --gpu_columns N: columns in flight (0 = device default) */
