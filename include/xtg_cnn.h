@@ -72,8 +72,9 @@ int xtc_net_train(xtc_net *net, const float *const *fbp, const float *const *icd
  * The network's inputs are the FBP image (xtg_init_object_fbp) and the
  * multi-resolution start (xtg_init_object_multires with coarse_iters coarse
  * iterations, z halved too when N_z is even and >= 16); its estimate is kept
- * (*used = 1) only if its MAP cost is below the multi-resolution start's
- * (both with e = y - Ax - d recomputed); otherwise the multi-resolution start
+ * (*used = 1) only if its MAP cost is below the multi-resolution start's by
+ * more than 1e-9 relative (both with e = y - Ax - d recomputed; the margin is
+ * the noise of the FP64 cost sums); otherwise the multi-resolution start
  * stays (*used = 0) -- the fallback.  ICD then continues at iteration 1.
  * Needs N_x, N_y, N_z multiples of 8. */
 struct xtg_ctx;
