@@ -21,6 +21,28 @@
 
 namespace xtg {
 
+// Footprint loads with L2 cache hints: e (re-read and updated through L2 by
+// other columns' reductions) is kept (evict_last), w (read once per visit) is
+// evicted first; neither is allocated in L1.
+__device__ __forceinline__ float4 ld_e(const float *p) {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  float4 v;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float4 ld_w(const float *p) {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  float4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p), "l"(pol));
+  return v;
+}
+
 // Footprint entries a thread loads before it uses any of them (table modes,
 // 16-byte rows): more loads in flight per warp to cover L2/HBM latency.
 #ifndef XTG_UNROLL
@@ -239,8 +261,8 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     auto accumulate = [&](int off, float a) {
       float ev[VEC], wv[VEC];
       if (VEC == 4) {
-        const float4 e4 = __ldcg(reinterpret_cast<const float4 *>(eb + off));
-        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wb + off));
+        const float4 e4 = ld_e(eb + off);
+        const float4 w4 = ld_w(wb + off);
         ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
         wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
       } else {
@@ -270,8 +292,8 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
           for (int u = 0; u < XTG_UNROLL; u++) en[u] = sEnt[e + u * vgs];
 #pragma unroll
           for (int u = 0; u < XTG_UNROLL; u++) {
-            e4[u] = __ldcg(reinterpret_cast<const float4 *>(eb + en[u].x));
-            w4[u] = __ldg(reinterpret_cast<const float4 *>(wb + en[u].x));
+            e4[u] = ld_e(eb + en[u].x);
+            w4[u] = ld_w(wb + en[u].x);
           }
 #pragma unroll
           for (int u = 0; u < XTG_UNROLL; u++) accumulate_vals(e4[u], w4[u], __int_as_float(en[u].y));
