@@ -79,9 +79,13 @@ __global__ void __launch_bounds__(FP_WARPS * 32) k_fp_bins(DevGeo G, FpArgs F) {
   const double lo = (double)G.R0 + (double)rb * G.delta_r - G.delta_xy - F.win_margin;
   const double hi = (double)G.R0 + (double)(rb + 32) * G.delta_r + G.delta_xy + F.win_margin;
   const int ta = lane, tb = lane + 32;  // this lane's rows (relative to t0)
+  // slices of those rows (detector row t belongs to slice t / zovl)
+  const bool va = ta < nt, vb = tb < nt;
+  const int za = (t0 + ta) / G.zovl, zb2 = (t0 + tb) / G.zovl;
   for (int j = 0; j < G.N_y; j++) {
     int klo, khi;
     if (!fp_col_range(G, cp, sp, xt_coord(G.y0, j, G.delta_xy), lo, hi, &klo, &khi)) continue;
+    const float *xrow = F.x + ((size_t)fr * G.N_y + j) * G.N_x * G.N_z;
     for (int kb = klo; kb <= khi; kb += 32) {
       const int k = kb + lane;
       float v[NS];
@@ -91,25 +95,35 @@ __global__ void __launch_bounds__(FP_WARPS * 32) k_fp_bins(DevGeo G, FpArgs F) {
       const int slo = max(0, rb - first), shi = min(n, rb + 32 - first);
       const unsigned hit = __ballot_sync(0xffffffffu, slo < shi);
       unsigned mk = hit;
+      // the z-line of the next hit column is loaded while the current one is added
+      float xa = 0.f, xb = 0.f;
+      if (mk) {
+        const float *xp = xrow + (size_t)(kb + __ffs(mk) - 1) * G.N_z;
+        xa = va ? __ldg(xp + za) : 0.f;
+        xb = vb ? __ldg(xp + zb2) : 0.f;
+      }
       while (mk) {
         const int l = __ffs(mk) - 1;
         mk &= mk - 1;
         const int fl = __shfl_sync(0xffffffffu, first, l);
         const int sl = __shfl_sync(0xffffffffu, slo, l), sh = __shfl_sync(0xffffffffu, shi, l);
-        const float *xp = F.x + (((size_t)fr * G.N_y + j) * G.N_x + (kb + l)) * G.N_z;
-        const float xa = ta < nt ? __ldg(xp + (t0 + ta) / G.zovl) : 0.f;
-        const float xb = tb < nt ? __ldg(xp + (t0 + tb) / G.zovl) : 0.f;
+        const float ca = xa, cb = xb;
+        if (mk) {
+          const float *xp = xrow + (size_t)(kb + __ffs(mk) - 1) * G.N_z;
+          xa = va ? __ldg(xp + za) : 0.f;
+          xb = vb ? __ldg(xp + zb2) : 0.f;
+        }
 #pragma unroll
         for (int s = 0; s < NS; s++) {
           const float a = __shfl_sync(0xffffffffu, v[s], l);
           if (s >= sl && s < sh && a != 0.f) {
             ACC *q = acc + (fl + s - rb) * 64;
             if (MODE <= 1) {
-              q[ta] = __fadd_rn(q[ta], __fmul_rn(xa, a));
-              q[tb] = __fadd_rn(q[tb], __fmul_rn(xb, a));
+              q[ta] = __fadd_rn(q[ta], __fmul_rn(ca, a));
+              q[tb] = __fadd_rn(q[tb], __fmul_rn(cb, a));
             } else {
-              q[ta] += (ACC)xa * (ACC)a;
-              q[tb] += (ACC)xb * (ACC)a;
+              q[ta] += (ACC)ca * (ACC)a;
+              q[tb] += (ACC)cb * (ACC)a;
             }
           }
         }
