@@ -48,6 +48,12 @@ WORKLOADS = {
     # up to 1 voxel/frame plus one growing; temporal prior weight 0.5
     "timbir4d": dict(N=256, NT=16, NP=1024, n_time=16, n_ell=8, mu=0.01, I0=1e4, zfrac=0.0, seed=3,
                      zinger=False, interlaced=(8, 256), moving=8),
+    # largest single-GPU 4D: 1024^2 x 64 voxels x 32 frames (8.6 GB FP32),
+    # 1536 bins (voxels 1.5 bins wide), 2 interlaced sub-frames of 64 views per
+    # frame (4096 views), 1e4 photons/ray, 0.5 % zingers with correction on,
+    # NHICD on; its sinogram is formed by the GPU projector (same A, same sums)
+    "timbir4d_large": dict(N=1024, NT=64, NP=4096, n_time=32, n_ell=8, mu=0.01, I0=1e4, zfrac=0.005, seed=5,
+                           zinger=True, interlaced=(2, 128), moving=8, dxy=1.5, gpu_fp=True),
 }
 WORKLOAD = WORKLOADS["plain3d"]
 METRIC = "voxel-updates/s (ICD)"
@@ -69,16 +75,22 @@ def sigma_t_arg(sigma_s_arg, delta_rtime, weight):
     return C_HU + SLOPE_HU * s / (delta_rtime * weight ** 0.5)
 
 
+def bins(w):
+    """Detector bins: voxels per side x voxel width in bins."""
+    return int(round(w["N"] * w.get("dxy", 1.0)))
+
+
 def params(w, radius=None):
-    N, nt = w["N"], w["n_time"]
+    nt, dxy = w["n_time"], w.get("dxy", 1.0)
+    NR = bins(w)
     rdelta = float(w["NP"] // nt)
     sig = 200000.0
     return xtg.Params(
         p=1.2, sigma_s=sig, sigma_t=sigma_t_arg(sig, rdelta, 0.5) if nt > 1 else sig, c_s=0.01, c_t=0.01,
-        delta_xy=1.0, delta_z=1.0, length_r=float(N), length_t=float(w["NT"]), rotation_center=N / 2.0, alpha=1.0,
-        Rtime0=0.0, Rtime_delta=rdelta, radius_obj=float(N) if radius is None else float(radius),
+        delta_xy=dxy, delta_z=1.0, length_r=float(NR), length_t=float(w["NT"]), rotation_center=NR / 2.0,
+        alpha=1.0, Rtime0=0.0, Rtime_delta=rdelta, radius_obj=float(NR) if radius is None else float(radius),
         zingerT=4.0 if w["zinger"] else 100000.0, zingerDel=0.5 if w["zinger"] else 0.0, iter=100, Rtime_num=nt,
-        num_projections=w["NP"], N_r=N, N_t=w["NT"], num_threads=1, positivity=1, no_NHICD=0)
+        num_projections=w["NP"], N_r=NR, N_t=w["NT"], num_threads=1, positivity=1, no_NHICD=0)
 
 
 def make_data(w):
@@ -90,7 +102,13 @@ def make_data(w):
     mv = w["moving"]
     x = xtg.phantom((w["n_time"], w["NT"], w["N"], w["N"]), w["n_ell"], w["mu"], w["seed"], n_moving=mv,
                     max_shift=1.0 if mv else 0.0, growing=1 if mv else 0)
-    ax = xtg.forward_cpu(p, t, a, x)
+    if w.get("gpu_fp"):
+        c = xtg.Context(p, t, a)
+        c.upload_object(x)
+        ax = c.forward_project()
+        c.close()
+    else:
+        ax = xtg.forward_cpu(p, t, a, x)
     y, wt = xtg.measure(ax, w["I0"], w["seed"] + 100, zinger_frac=w["zfrac"])
     return p, t, a, x, y, wt
 
@@ -158,7 +176,7 @@ def workload(args):
 
 
 def base_config(w, amode):
-    return {"workload": workload_name(w), "N_xy": w["N"], "N_z": w["NT"], "N_time": w["n_time"], "N_r": w["N"],
+    return {"workload": workload_name(w), "N_xy": w["N"], "N_z": w["NT"], "N_time": w["n_time"], "N_r": bins(w),
             "N_t": w["NT"], "N_p": w["NP"], "views": "interlaced K=%d N_theta=%d" % w["interlaced"]
             if w["interlaced"] else "uniform", "zinger": [4.0, 0.5] if w["zinger"] else None,
             "zinger_frac": w["zfrac"], "temporal_weight": 0.5 if w["n_time"] > 1 else None, "nhicd": True,
@@ -294,17 +312,19 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     return out
 
 
-def nnz_per_column(ctx, n_cols=512, seed=0):
-    """Average A-matrix entries per column over all views (sampled columns)."""
+def nnz_per_column(ctx, p, t, a, n_cols=512, seed=0):
+    """Average A-matrix entries of a column over the views of its frame
+    (sampled columns, frame 0; every frame has the same number of views)."""
     rng = np.random.default_rng(seed)
     g = ctx.geometry()
+    views = np.nonzero(xtg.host_geometry(p, t, a)[3] == 0)[0]
     rows = rng.integers(0, ctx.N_y, n_cols)
     cols = rng.integers(0, ctx.N_x, n_cols)
     keep = [(r, c) for r, c in zip(rows, cols)
             if ((g.x0 + (c + 0.5) * g.delta_xy) ** 2 + (g.y0 + (r + 0.5) * g.delta_xy) ** 2) < g.radius_obj ** 2]
-    rr = np.repeat([k[0] for k in keep], ctx.N_p)
-    cc = np.repeat([k[1] for k in keep], ctx.N_p)
-    vv = np.tile(np.arange(ctx.N_p), len(keep))
+    rr = np.repeat([k[0] for k in keep], len(views))
+    cc = np.repeat([k[1] for k in keep], len(views))
+    vv = np.tile(views, len(keep))
     _, _, cnt = ctx.amatrix(rr, cc, vv)
     return float(cnt.sum()) / len(keep)
 
@@ -349,7 +369,7 @@ def run_ours(args):
     tf = time.perf_counter()
     ctx.init_error_sino()  # e = y - Ax - d (fast projector), timed once for the log
     fp_ms = (time.perf_counter() - tf) * 1e3
-    nnz = nnz_per_column(ctx)
+    nnz = nnz_per_column(ctx, p, t, a)
     it = 0
     for _ in range(args.warmup):
         it += 1
