@@ -21,6 +21,15 @@
 
 namespace xtg {
 
+// Work items of at most XTG_SMALL_ROWS detector rows run in CTAs of
+// XTG_SMALL_NT threads (table modes, parallel schedule).
+#ifndef XTG_SMALL_ROWS
+#define XTG_SMALL_ROWS 16
+#endif
+#ifndef XTG_SMALL_NT
+#define XTG_SMALL_NT 64
+#endif
+
 // Footprint loads with L2 cache hints: e (re-read and updated through L2 by
 // other columns' reductions) is kept (evict_last), w (read once per visit) is
 // evicted first; neither is allocated in L1.
@@ -86,8 +95,12 @@ __device__ __forceinline__ Nbr nbr_term(const DevGeo &G, const float *sNb, const
   return o;
 }
 
-template <int VEC, int AMODE, int SEQ, int AS>
-__global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArgs A, int vmax, int zmax) {
+// NT threads per CTA: 256 for long z-lines; 64 where a work item is short
+// (few detector rows), so the per-item fixed work (neighbourhood, A staging,
+// barriers, the surrogate step) runs in four times as many CTAs at once.
+template <int VEC, int AMODE, int SEQ, int AS, int NT = XTG_THREADS>
+__global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_columns(DevGeo G, IcdArgs A, int vmax,
+                                                                                 int zmax) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // AMODE 0 (A computed here): per view {first | n << 24, view index, AS values}
   int *sPack = reinterpret_cast<int *>(smem_raw);        // [vmax]
@@ -104,7 +117,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
   float *sDelta = sTn + 2 * zmax;                         // [zmax]
 
   __shared__ int sItem;
-  __shared__ double sAbs[XTG_THREADS / 32];
+  __shared__ double sAbs[NT / 32];
   __shared__ unsigned sUpd, sZero;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -140,7 +153,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     // 1. neighbourhood: the 3x3 columns' z-lines over [zb-1, ze+1], and the
     //    same column in frames fr-1 and fr+1 (0 outside the volume)
     const size_t plane = (size_t)G.N_y * G.N_x;
-    for (int k = tid; k < 9 * (Z + 2); k += XTG_THREADS) {
+    for (int k = tid; k < 9 * (Z + 2); k += NT) {
       const int c = k / (Z + 2), zz = k - c * (Z + 2);
       const int jj = row + c / 3 - 1, kk = col + c % 3 - 1, za = zb - 1 + zz;
       float v = 0.f;
@@ -148,7 +161,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
         v = A.x[(((size_t)fr * plane) + (size_t)jj * G.N_x + kk) * G.N_z + za];
       sNb[c * (zmax + 2) + zz] = v;
     }
-    for (int k = tid; k < 2 * Z; k += XTG_THREADS) {
+    for (int k = tid; k < 2 * Z; k += NT) {
       const int s = k / Z, z = k - s * Z, f2 = fr + (s ? 1 : -1);
       float v = 0.f;
       if (f2 >= 0 && f2 < G.N_time) v = A.x[(((size_t)f2 * plane) + (size_t)row * G.N_x + col) * G.N_z + zb + z];
@@ -162,19 +175,19 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     // the same test and the e update has nothing to add).
     bool quiet = A.iter > 1;
     if (quiet) {
-      for (int k = tid; k < 9 * (Z + 2); k += XTG_THREADS) {
+      for (int k = tid; k < 9 * (Z + 2); k += NT) {
         const int c = k / (Z + 2), zz = k - c * (Z + 2);
         const float v = sNb[c * (zmax + 2) + zz];
         const bool self = (c == 4) && zz >= 1 && zz <= Z;
         if (self ? (v != 0.f) : (v > 0.f)) quiet = false;
       }
-      for (int k = tid; k < 2 * Z; k += XTG_THREADS)
+      for (int k = tid; k < 2 * Z; k += NT)
         if (sTn[(k / Z) * zmax + k % Z] > 0.f) quiet = false;
     }
     const bool skip_all = __syncthreads_and(quiet) != 0;
     // 2. the column's A entries (times delta_t, XT_VoxUpdate.c:27) -> smem
     if (AMODE == 0 && !skip_all) {
-      for (int v = tid; v < V; v += XTG_THREADS) {
+      for (int v = tid; v < V; v += NT) {
         const int p = A.view_idx[vs + v];
         float vals[AS];
         int first;
@@ -192,7 +205,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
       const long long s0 = A.tstart[ti];
       ne = (int)(A.tstart[ti + 1] - s0);
       const float sc = (AMODE == 1) ? A.tscale[ti] : 1.f;
-      for (int e = tid; e < ne; e += XTG_THREADS) {
+      for (int e = tid; e < ne; e += NT) {
         const float a = (AMODE == 2) ? __ldg(A.tval32 + s0 + e) : __half2float(A.tval16[s0 + e]) * sc;
         sEnt[e] = make_int2(__ldg(A.toff + s0 + e), __float_as_int(a));
       }
@@ -203,7 +216,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     const int tln = (T + VEC - 1) / VEC;
     int tlp = 1;
     while (tlp < tln) tlp <<= 1;
-    const int vgs = XTG_THREADS / tlp, tl = tid & (tlp - 1), vg = tid / tlp;
+    const int vgs = NT / tlp, tl = tid & (tlp - 1), vg = tid / tlp;
     float th1[VEC], th2[VEC];
 #pragma unroll
     for (int c = 0; c < VEC; c++) th1[c] = th2[c] = 0.f;
@@ -325,10 +338,10 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
       }
     }
     __syncthreads();
-    for (int t = tid; t < T; t += XTG_THREADS) {
+    for (int t = tid; t < T; t += NT) {
       float s1 = 0.f, s2 = 0.f;
 #pragma unroll
-      for (int wq = 0; wq < XTG_THREADS / 32; wq++) {  // every warp wrote its partial (zeros if idle)
+      for (int wq = 0; wq < NT / 32; wq++) {  // every warp wrote its partial (zeros if idle)
         s1 += sRed[wq * 128 + t];
         s2 += sRed[8 * 128 + wq * 128 + t];
       }
@@ -388,7 +401,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
       for (int par = 0; par < 2; par++) {
         const int zfirst = ((zb & 1) == par) ? 0 : 1;  // first z (relative) with absolute parity par
         const int nvox = (Z - zfirst + 1) / 2;
-        for (int s0 = 0; s0 < nvox; s0 += XTG_THREADS / 8) {
+        for (int s0 = 0; s0 < nvox; s0 += NT / 8) {
           const int vi = s0 + slot;
           const bool act = vi < nvox;
           const int z = zfirst + 2 * (act ? vi : 0);
@@ -456,7 +469,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
 
     // 5. MagUpdateMap[frame][block][row][col] = sum |delta| over the block's
     //    slices of this visit (XT_VoxUpdate.c:128, 236); sum |x| and counters
-    for (int b = tid; b < G.nzb; b += XTG_THREADS) {
+    for (int b = tid; b < G.nzb; b += NT) {
       const int bz0 = b * G.zstep, bz1 = (b >= G.nzb - 1) ? G.N_z - 1 : (b + 1) * G.zstep - 1;
       const int lo = max(bz0, zb), hi = min(bz1, ze);
       float *mp = A.magmap + (((size_t)fr * G.nzb + b) * G.N_y + row) * G.N_x + col;
@@ -478,7 +491,7 @@ __global__ void __launch_bounds__(XTG_THREADS, 4) k_icd_columns(DevGeo G, IcdArg
     __syncthreads();
     if (tid == 0) {
       double s = 0.0;
-      for (int wq = 0; wq < XTG_THREADS / 32; wq++) s += sAbs[wq];
+      for (int wq = 0; wq < NT / 32; wq++) s += sAbs[wq];
       atomicAdd(&A.st_absx[blockIdx.x & 63], s);
       atomicAdd(&A.st_cnt[0], (unsigned long long)sUpd);
       atomicAdd(&A.st_cnt[1], (unsigned long long)sZero);
@@ -546,9 +559,11 @@ typedef void (*IcdKernel)(DevGeo, IcdArgs, int, int);
 // A computed in the kernel (amode 0): slot count 3 covers delta_xy <= delta_r,
 // 4 covers delta_xy <= 1.5 delta_r, 12 covers delta_xy <= 5.5 delta_r.  The
 // table modes (1 = FP16, 2 = FP32) have no per-view slots.
-static IcdKernel icd_kernel(int vec, int amode, int seq, int as) {
+static IcdKernel icd_kernel(int vec, int amode, int seq, int as, int nt) {
 #define XTG_K(V, S) (as == 3 ? k_icd_columns<V, 0, S, 3> : as == 4 ? k_icd_columns<V, 0, S, 4> : k_icd_columns<V, 0, S, 12>)
 #define XTG_T(V, M, S) k_icd_columns<V, M, S, 3>
+  if (nt != XTG_THREADS && vec == 4 && amode != 0 && !seq)  // short items, table modes
+    return amode == 1 ? k_icd_columns<4, 1, 0, 3, XTG_SMALL_NT> : k_icd_columns<4, 2, 0, 3, XTG_SMALL_NT>;
   if (vec == 4) {
     if (amode == 0) return seq ? XTG_K(4, 1) : XTG_K(4, 0);
     if (amode == 1) return seq ? XTG_T(4, 1, 1) : XTG_T(4, 1, 0);
@@ -580,10 +595,16 @@ cudaError_t launch_magmap_zero(const DevGeo &G, const IcdArgs &A, int grid, cuda
   return cudaGetLastError();
 }
 
+// threads per CTA for items of zmax slices: XTG_SMALL_NT for short table-mode items
+int icd_threads(int vec, int amode, int seq, int zmax, int zovl) {
+  return (vec == 4 && amode != 0 && !seq && zmax * zovl <= XTG_SMALL_ROWS) ? XTG_SMALL_NT : XTG_THREADS;
+}
+
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st) {
   const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as, amode, vec);
-  IcdKernel k = icd_kernel(vec, amode, seq, as);
+  const int nt = icd_threads(vec, amode, seq, zmax, G.zovl);
+  IcdKernel k = icd_kernel(vec, amode, seq, as, nt);
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   // e and w stream through L2 (e must, it is updated by other CTAs' atomics),
@@ -591,18 +612,19 @@ cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, in
   e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributePreferredSharedMemoryCarveout,
                            (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<grid, XTG_THREADS, smem, st>>>(G, A, vmax, zmax);
+  k<<<grid, nt, smem, st>>>(G, A, vmax, zmax);
   return cudaGetLastError();
 }
 
 int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl) {
   const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as, amode, vec);
-  IcdKernel k = icd_kernel(vec, amode, seq, as);
+  const int nt = icd_threads(vec, amode, seq, zmax, zovl);
+  IcdKernel k = icd_kernel(vec, amode, seq, as, nt);
   int nb = 0;
   cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute((const void *)k, cudaFuncAttributePreferredSharedMemoryCarveout,
                        (int)cudaSharedmemCarveoutMaxShared);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)k, XTG_THREADS, smem) != cudaSuccess) return 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)k, nt, smem) != cudaSuccess) return 1;
   return nb > 0 ? nb : 1;
 }
 
