@@ -162,12 +162,18 @@ int xtg_upsample(xtg_ctx *ctx, const float *in, float *out, int32_t nt, int32_t 
 
 /* Multi-resolution start, the launcher's coarse-to-fine stages in one call:
  * reconstruct the same data on a grid with voxels twice as large in x-y (and
- * z with with_z), from its FBP image, for coarse_iters ICD iterations; then
- * object := that reconstruction upsampled as above (0 outside the disk,
- * clamped with positivity) and e = y - Ax - d.  The coarse context is kept
- * for later calls.  No XT_Engine counterpart (the launcher runs the stages
- * as separate XT_Engine processes with --initICD 2/3). */
-int xtg_init_object_multires(xtg_ctx *ctx, int32_t coarse_iters, int32_t with_z);
+ * z with XTG_MULTIRES_Z), from its FBP image, for coarse_iters ICD
+ * iterations; then object := that reconstruction upsampled as above (0
+ * outside the disk, clamped with positivity) and e = y - Ax - d.  With
+ * XTG_MULTIRES_BIN the coarse grid sees a detector binned 2x in bins (and
+ * rows with XTG_MULTIRES_Z): weights summed, projections weight-averaged --
+ * the binning genSinogram_subsampleCounts (XT_genSinogram.c:303-374) applies
+ * to counts -- four times fewer sinogram entries per coarse iteration.  The
+ * coarse context is kept for later calls with the same flags.  No XT_Engine
+ * counterpart (the launcher runs the stages as separate XT_Engine processes
+ * with --initICD 2/3). */
+enum { XTG_MULTIRES_Z = 1, XTG_MULTIRES_BIN = 2 };
+int xtg_init_object_multires(xtg_ctx *ctx, int32_t coarse_iters, int32_t flags);
 /* e = y - A x - d with FP64 accumulation, rounded to FP32: the periodic
  * resync that removes the drift of incremental FP32 updates.  The same pass
  * yields the MAP cost of the current object in FP64 (outputs may be NULL). */

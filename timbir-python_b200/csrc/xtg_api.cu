@@ -51,6 +51,8 @@ void xtg_set_error_text(const char *msg) { snprintf(g_err, sizeof g_err, "%s", m
   } while (0)
 
 #define NSLOT 64
+// parallel ICD: at most 1 in XTG_CONC_DIV of the columns updated at once
+#define XTG_CONC_DIV 32
 
 struct xtg_ctx {
   xt_params prm;
@@ -89,6 +91,7 @@ struct xtg_ctx {
   long long l2_bytes = 0;
   std::vector<double> t_in, a_in;  // view times / angles as given (for the coarse context)
   xtg_ctx *coarse = nullptr;      // multi-resolution start: the 2x coarser grid
+  int coarse_flags = 0;           // the XTG_MULTIRES_* flags it was built for
   int zslab_req = 0;  // z slices per ICD work piece; 0 = from the L2 size
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
@@ -935,35 +938,87 @@ int xtg_upsample(xtg_ctx *c, const float *in, float *out, int32_t nt, int32_t nz
   return rc;
 }
 
-int xtg_init_object_multires(xtg_ctx *c, int32_t coarse_iters, int32_t with_z) {
-  if (!c || coarse_iters < 0) return XTG_E_ARG;
+// 2 x 2 (or 2 x 1) detector binning for the binned coarse problem: weights
+// add (as counts do, genSinogram_subsampleCounts, XT_genSinogram.c:303-374, sums them),
+// the projection is the weight-averaged one, the offset the plain mean
+__global__ void k_bin_sino(int np, int nrc, int ntc, int nrf, int ntf, int fr, int ft, const float *y, const float *w,
+                           const float *d, float *yc, float *wc, float *dc) {
+  const long long n = (long long)np * nrc * ntc;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i % ntc);
+    const long long q = i / ntc;
+    const int r = (int)(q % nrc), p = (int)(q / nrc);
+    double W = 0, WY = 0, Y = 0, D = 0;
+    for (int a = 0; a < fr; a++)
+      for (int b = 0; b < ft; b++) {
+        const size_t f = ((size_t)p * nrf + r * fr + a) * ntf + t * ft + b;
+        W += w[f];
+        WY += (double)w[f] * y[f];
+        Y += y[f];
+        if (p == 0) D += d[(size_t)(r * fr + a) * ntf + t * ft + b];
+      }
+    wc[i] = (float)W;
+    yc[i] = (float)(W > 0 ? WY / W : Y / (fr * ft));
+    if (p == 0) dc[(size_t)r * ntc + t] = (float)(D / (fr * ft));
+  }
+}
+
+int xtg_init_object_multires(xtg_ctx *c, int32_t coarse_iters, int32_t flags) {
+  if (!c || coarse_iters < 0 || (flags & ~(XTG_MULTIRES_Z | XTG_MULTIRES_BIN))) return XTG_E_ARG;
   if (!c->have_sino) {
     set_err("xtg_init_object_multires: no sinogram uploaded");
     return XTG_E_STATE;
   }
   const xt_geom &g = c->g;
+  // a counts-ingested sinogram (sinobin 3) is already binned to the voxel
+  // size, so its coarse stage bins it further, as the reference's counts
+  // ingest does at each stage of the launcher
+  if (c->prm.sinobin == 3) flags |= XTG_MULTIRES_BIN;
+  const bool with_z = flags & XTG_MULTIRES_Z, bin = flags & XTG_MULTIRES_BIN;
   if (g.N_x % 2 || g.N_y % 2 || (with_z && g.N_z % 2)) {
     set_err("xtg_init_object_multires: grid not divisible by 2");
     return XTG_E_ARG;
   }
-  if (c->coarse && (c->coarse->g.N_z == g.N_z) != !with_z) {
+  if (c->coarse && c->coarse_flags != flags) {
     xtg_destroy(c->coarse);
     c->coarse = nullptr;
   }
   if (!c->coarse) {
-    // the same scan with voxels twice as large (the launcher's coarser stage)
+    // the same scan with voxels twice as large (the launcher's coarser
+    // stage); binned, its detector bins (and rows) are twice as large too,
+    // the geometry counts ingest derives (sinobin 3: N_r / delta_xy bins of
+    // delta_xy fine bins, priors scaled by delta_xy as on the unbinned grid)
     xt_params cp = c->prm;
     cp.delta_xy *= 2;
     if (with_z) cp.delta_z *= 2;
+    if (bin) cp.sinobin = 3;
     int rc = xtg_create(&cp, c->t_in.data(), c->a_in.data(), (int32_t)c->t_in.size(), &c->coarse);
     if (rc) return rc;
+    c->coarse_flags = flags;
     if ((rc = xtg_set_options(c->coarse, c->a_mode, XTG_ORDER_PARALLEL, c->max_columns, c->seed))) return rc;
   }
   xtg_ctx *cc = c->coarse;
-  // the same measurement, weights (already scaled by the variance) and offset
-  CK(cudaMemcpyAsync(cc->d_y, c->d_y, c->ns * 4, cudaMemcpyDeviceToDevice, c->st));
-  CK(cudaMemcpyAsync(cc->d_w, c->d_w, c->ns * 4, cudaMemcpyDeviceToDevice, c->st));
-  CK(cudaMemcpyAsync(cc->d_d, c->d_d, c->nrt * 4, cudaMemcpyDeviceToDevice, c->st));
+  // fine detector bins (rows) per coarse one: 2 binned from voxel-sized bins,
+  // 2 delta_xy (2 delta_z) from bins of a grid with delta_xy > 1
+  const int fr = g.N_r / cc->g.N_r, ft = g.N_t / cc->g.N_t;
+  if (cc->g.N_x * 2 != g.N_x || cc->g.N_y * 2 != g.N_y || cc->g.N_z * (with_z ? 2 : 1) != g.N_z ||
+      cc->g.N_p != g.N_p || cc->g.N_r * fr != g.N_r || cc->g.N_t * ft != g.N_t || (!bin && (fr != 1 || ft != 1))) {
+    set_err("xtg_init_object_multires: the coarse grid is not half the fine one");
+    return XTG_E_ARG;
+  }
+  if (bin) {
+    // the binned measurement; weights are already scaled by the variance
+    const unsigned gr = (unsigned)std::min<size_t>((cc->ns + 255) / 256, (size_t)c->sm_count * 16);
+    k_bin_sino<<<gr, 256, 0, c->st>>>(g.N_p, cc->g.N_r, cc->g.N_t, g.N_r, g.N_t, fr, ft, c->d_y, c->d_w, c->d_d,
+                                      cc->d_y, cc->d_w, cc->d_d);
+    c->launches++;
+    CK(cudaGetLastError());
+  } else {
+    // the same measurement, weights (already scaled by the variance) and offset
+    CK(cudaMemcpyAsync(cc->d_y, c->d_y, c->ns * 4, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(cc->d_w, c->d_w, c->ns * 4, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(cc->d_d, c->d_d, c->nrt * 4, cudaMemcpyDeviceToDevice, c->st));
+  }
   CK(cudaMemcpyAsync(cc->d_var, c->d_var, 4, cudaMemcpyDeviceToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   cc->have_sino = 1;
@@ -1380,6 +1435,14 @@ static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, c
   } else {
     const int occ = icd_occupancy(vec, amode, 0, as, vcap, zmax, g.zovl);
     grid = c->sm_count * occ;
+    // Columns updated at the same time read each other's stale error
+    // sinogram; near neighbours share most of their footprint, so too many
+    // of them at once overshoot (Jacobi-like) and the cost stops falling.
+    // At most 1 in XTG_CONC_DIV of the grid's columns is in flight: on a
+    // 32^2-column grid 64 and more at once left the cost oscillating 20-50 %
+    // above the converged value, 32 did not; grids of 256^2 columns and up
+    // keep every resident CTA busy.
+    grid = std::min(grid, std::max(8, (int)(((long long)g.N_time * c->n_masked) / XTG_CONC_DIV)));
     if (c->max_columns > 0) grid = std::min(grid, c->max_columns);
     if (!n_dev) grid = std::min(grid, std::max(n * nsub, 1));
   }

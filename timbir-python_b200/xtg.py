@@ -22,6 +22,7 @@ LIBDIR = os.path.join(HERE, "lib")
 
 XTG_A_FP32, XTG_A_FP16, XTG_A_TABLE32, XTG_A_AUTO = 0, 1, 2, 3
 XTG_ORDER_PARALLEL, XTG_ORDER_SEQUENTIAL = 0, 1
+XTG_MULTIRES_Z, XTG_MULTIRES_BIN = 1, 2
 
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
@@ -299,8 +300,12 @@ class Context:
         _check(self.lib.xtg_upsample(self.h, _p(a), _p(out), nt, nz, ny, nx, int(with_z)), "xtg_upsample")
         return out
 
-    def init_multires(self, coarse_iters=40, with_z=True):
-        _check(self.lib.xtg_init_object_multires(self.h, int(coarse_iters), int(with_z)), "xtg_init_object_multires")
+    def init_multires(self, coarse_iters=40, with_z=True, binned=False):
+        """Multi-resolution start: coarse_iters ICD iterations on the grid with
+        voxels twice as large (x-y, and z when with_z), upsampled; binned runs
+        them against the detector binned to the coarse voxel size."""
+        flags = (XTG_MULTIRES_Z if with_z else 0) | (XTG_MULTIRES_BIN if binned else 0)
+        _check(self.lib.xtg_init_object_multires(self.h, int(coarse_iters), flags), "xtg_init_object_multires")
 
     def object_to_device(self, dst):
         _check(self.lib.xtg_object_to_device(self.h, WarmNet._dev(dst)), "xtg_object_to_device")
