@@ -1,6 +1,10 @@
 """The warm-start network's tcgen05 implicit-GEMM convolutions against a plain
 PyTorch fp32 reference on the CPU (same BF16-rounded inputs and weights).
 
+Both kernels are covered: the gather kernel (operands gathered per K stage)
+and the tile kernel (the input tile staged once by TMA, each tap a shifted
+shared-memory view; X a multiple of 128, Z even, cout <= 64).
+
 Tolerance: FP32 accumulation in a different order over K = 27*cin terms,
 |got - ref| <= 1e-4 * max|ref| (FP32 output), plus one BF16 rounding of the
 result (2^-8 relative) for BF16 outputs.
@@ -22,6 +26,16 @@ SHAPES = [  # nb, Y, X, Z, cin, cout
     (1, 16, 16, 8, 64, 32),
     (1, 8, 8, 16, 160, 64),
 ]
+
+
+TILE_SHAPES = [  # nb, Y, X, Z, cin, cout: 16-channel chunks, a half chunk, batches, tile edges
+    (1, 3, 128, 4, 32, 32),
+    (2, 2, 128, 6, 48, 64),
+    (1, 2, 256, 2, 8, 16),
+    (1, 3, 128, 4, 80, 32),
+    (1, 2, 128, 2, 24, 48),
+]
+GATHER, TILE, AUTO = 1, 2, 0
 
 
 def kpad(cin):
@@ -116,3 +130,67 @@ def test_conv_weight_gradient(shape):
     check(lib.xtc_conv3d_wgrad(ptr(xd), ptr(dyd), ptr(dw), nb, Y, X, Z, cin, cout))
     got = dw.cpu()
     assert torch.max(torch.abs(got - ref_rows)) <= 1e-4 * torch.max(torch.abs(ref_rows))
+
+
+def conv_path(lib, xd, wd, bd, out, shape, epi, sign, path):
+    nb, Y, X, Z, cin, cout = shape
+    return lib.xtc_conv3d_path(ptr(xd), ptr(wd), ptr(bd) if bd is not None else None, ptr(out), nb, Y, X, Z, cin,
+                               cout, kpad(cin), epi, sign, path)
+
+
+@pytest.mark.parametrize("shape", TILE_SHAPES)
+def test_tile_conv_forward(shape):
+    lib = xtg.gpu_lib()
+    nb, Y, X, Z, cin, cout = shape
+    x, w, b = case(shape, 3)
+    ref = F.conv3d(x, w, padding=1)
+    xd = to_cl(x).to(torch.bfloat16).cuda()
+    wd = pack_w(w).cuda()
+    bd = b.float().cuda()
+    out = torch.empty(nb, Y, X, Z, cout, dtype=torch.float32, device="cuda")
+    check(conv_path(lib, xd, wd, bd, out, shape, 2, 1, TILE))
+    got = from_cl(out.cpu())
+    assert torch.max(torch.abs(got - ref)) <= 1e-4 * torch.max(torch.abs(ref))
+    # the automatic choice is the tile kernel: the same sums in the same order
+    out2 = torch.empty_like(out)
+    check(conv_path(lib, xd, wd, bd, out2, shape, 2, 1, AUTO))
+    assert torch.equal(out, out2)
+    refr = torch.relu(ref + b.view(1, -1, 1, 1, 1))
+    tol = 1e-4 * torch.max(torch.abs(refr)) + 2 ** -8 * torch.max(torch.abs(refr))
+    for epi, want in ((0, refr), (1, ref)):
+        outb = torch.empty(nb, Y, X, Z, cout, dtype=torch.bfloat16, device="cuda")
+        check(conv_path(lib, xd, wd, bd, outb, shape, epi, 1, TILE))
+        assert torch.max(torch.abs(from_cl(outb.float().cpu()) - want)) <= tol + 2 ** -8 * torch.max(torch.abs(want))
+    # and the gather kernel agrees with it
+    outg = torch.empty_like(out)
+    check(conv_path(lib, xd, wd, bd, outg, shape, 2, 1, GATHER))
+    assert torch.max(torch.abs(outg - out)).item() <= 1e-5 * torch.max(torch.abs(ref)).item()
+
+
+@pytest.mark.parametrize("shape", [s for s in TILE_SHAPES if s[4] % 16 == 0 and s[4] <= 64])
+def test_tile_conv_input_gradient(shape):
+    lib = xtg.gpu_lib()
+    nb, Y, X, Z, cin, cout = shape
+    x, w, b = case(shape, 4)
+    g = torch.Generator().manual_seed(8)
+    dy = torch.randn(nb, cout, Y, X, Z, generator=g).to(torch.bfloat16).float()
+    ref = torch.nn.grad.conv3d_input(x.shape, w, dy, padding=1)
+    wtd = pack_w(w.permute(1, 0, 2, 3, 4).contiguous()).cuda()
+    dyd = to_cl(dy).to(torch.bfloat16).cuda()
+    out = torch.empty(nb, Y, X, Z, cin, dtype=torch.float32, device="cuda")
+    check(lib.xtc_conv3d_path(ptr(dyd), ptr(wtd), None, ptr(out), nb, Y, X, Z, cout, cin, kpad(cout), 2, -1, TILE))
+    got = from_cl(out.cpu())
+    assert torch.max(torch.abs(got - ref)) <= 1e-4 * torch.max(torch.abs(ref))
+
+
+def test_tile_conv_rejects_unsupported_shapes():
+    lib = xtg.gpu_lib()
+    shape = (1, 2, 96, 4, 32, 32)  # X not a multiple of 128
+    x, w, b = case(shape)
+    xd = to_cl(x).to(torch.bfloat16).cuda()
+    wd = pack_w(w).cuda()
+    out = torch.empty(1, 2, 96, 4, 32, dtype=torch.float32, device="cuda")
+    assert conv_path(lib, xd, wd, None, out, shape, 2, 1, TILE) == -1  # XTG_E_ARG
+    check(conv_path(lib, xd, wd, None, out, shape, 2, 1, AUTO))
+    assert torch.max(torch.abs(from_cl(out.cpu()) - F.conv3d(x, w, padding=1))) <= 1e-4 * float(
+        torch.max(torch.abs(F.conv3d(x, w, padding=1))))

@@ -42,7 +42,7 @@ def random_params(net, seed):
     return p
 
 
-@pytest.mark.parametrize("shape", [(2, 16, 16, 16), (1, 32, 16, 8)])
+@pytest.mark.parametrize("shape", [(2, 16, 16, 16), (1, 32, 16, 8), (1, 16, 128, 8)])
 def test_forward_and_gradients_match_reference(shape):
     net = xtg.WarmNet(seed=3)
     p = random_params(net, 5)

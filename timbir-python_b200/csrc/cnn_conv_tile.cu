@@ -1,0 +1,259 @@
+// cnn_conv_tile.cu -- 3x3x3 convolutions of the warm-start network on tiles
+// staged once by TMA (BF16 in, FP32 accumulation in TMEM).
+//
+// The gather kernel in cnn_conv.cu builds every A row (voxel x 64 K values)
+// with per-thread loads: each input voxel is fetched 27 times.  Here a CTA
+// owns an output tile of 128 x-voxels x TZ z-lines of one y-row; TMA stages
+// the tile's input halo (130 x (TZ + 2) x 3 voxels, 16 channels per stage,
+// zero filled outside the volume) in shared memory once, laid out as two
+// 8-channel planes, x fastest:  row r = (y' * TZS + z') * TXS + x'.  In that
+// layout the A operand of tap (dy, dx, dz) for output line z is the run of 128
+// rows starting at r0(z) + (dy * TZS + dz) * TXS + dx -- one shared-memory
+// descriptor with a shifted start address (K-major, no swizzle: 16-byte rows,
+// 8-row core matrices 128 bytes apart, the two 8-channel halves of an MMA one
+// plane apart).  No im2col gather is ever materialised.
+//
+// Weights come pre-packed per 16-channel chunk as Wp[chunk][tap][half][n][8]
+// (the canonical K-major B layout of one MMA per tap) and are copied with one
+// bulk copy per stage.  One thread issues the TMA, the bulk copies and all
+// MMAs; stages are double-buffered so the copies for chunk c + 1 overlap the
+// MMAs of chunk c.  Every wait is bounded and reports through *err.
+//
+// Shapes: X a multiple of 128, Z even, cin a multiple of 8, cout a multiple of
+// 16 up to 64 (shared memory: 2 x (49,920 + 864 cout) bytes, one stage for
+// cin <= 16).  Other shapes use the gather kernel.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "cnn_tc.cuh"
+#include "xtg_cnn_internal.h"
+
+namespace xtc {
+
+namespace {
+
+constexpr int TX = 128, TXS = TX + 2;  // output x-voxels per tile, staged with one halo each side
+constexpr int TZ = 2, TZS = TZ + 2;    // output z-lines per tile
+constexpr int TROWS = 3 * TZS * TXS;   // staged voxels (rows) per 8-channel plane
+constexpr uint32_t TPLANE = TROWS * 16;
+constexpr uint32_t TA_STAGE = 2 * TPLANE;  // 16 channels
+constexpr int TN_MAX = 64;
+static_assert(TPLANE % 128 == 0, "TMA destinations must stay 128-byte aligned");
+
+__host__ __device__ constexpr uint32_t b_stage_bytes(int n) { return 27u * (uint32_t)n * 32u; }
+
+template <int SIGN, int EPI>
+__global__ void __launch_bounds__(128, 1)
+    k_conv_tile(const __grid_constant__ CUtensorMap tin, ConvShape s, const __nv_bfloat16 *__restrict__ wp,
+                const float *__restrict__ bias, void *out, int *err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const int N = s.n;
+  const uint32_t B_STAGE = b_stage_bytes(N);
+  const int nchunk = (s.cin + 15) >> 4;
+  uint8_t *sA = sm, *sB = sm + (nchunk > 1 ? 2 : 1) * TA_STAGE;
+  __shared__ uint64_t full[2], empty[2], done;
+  __shared__ uint32_t tbase;
+  __shared__ int bad;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int x0 = blockIdx.x * TX, z0 = blockIdx.y * TZ;
+  const int y = blockIdx.z % s.Y, b = blockIdx.z / s.Y;
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], 1);
+    mbar_init(&empty[1], 1);
+    mbar_init(&done, 1);
+    mbar_init_fence();
+    bad = 0;
+  }
+  if (warp == 0) tmem_alloc(&tbase, tmem_cols(TZ * N));
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tbase;
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(N, 0, 0);
+      const long long lim = 1ll << 24;
+      int issued[2] = {0, 0}, landed[2] = {0, 0};
+      auto load = [&](int c) {
+        const int st = c & 1;
+        uint8_t *a = sA + st * TA_STAGE;
+        mbar_expect_tx(&full[st], TA_STAGE + B_STAGE);
+        // channels 16c .. 16c + 7 and 16c + 8 .. 16c + 15 (past cin: zero fill)
+        tma_load_5d(a, &tin, 16 * c, x0 - 1, z0 - 1, y - 1, b, &full[st]);
+        tma_load_5d(a + TPLANE, &tin, 16 * c + 8, x0 - 1, z0 - 1, y - 1, b, &full[st]);
+        bulk_load(sB + st * B_STAGE, wp + (size_t)c * (B_STAGE / 2), B_STAGE, &full[st]);
+        issued[st]++;
+      };
+      bool ok = true;
+      load(0);
+      if (nchunk > 1) load(1);
+      for (int c = 0; c < nchunk; c++) {
+        const int st = c & 1;
+        if (!mbar_wait(&full[st], (uint32_t)(c >> 1) & 1u, lim)) {
+          ok = false;
+          break;
+        }
+        landed[st]++;
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(sA + st * TA_STAGE), b0 = smem_u32(sB + st * B_STAGE);
+        for (int t = 0; t < 27; t++) {
+          const int dy = SIGN * (t / 9 - 1), dx = SIGN * ((t / 3) % 3 - 1), dz = SIGN * (t % 3 - 1);
+          const int shift = (dy * TZS + dz) * TXS + dx;
+          const uint64_t db = sdesc(b0 + (uint32_t)t * N * 32, (uint32_t)N * 16, 128);
+#pragma unroll
+          for (int zo = 0; zo < TZ; zo++) {
+            const int r = (TZS + zo + 1) * TXS + 1 + shift;  // output line (y, z0 + zo), x = x0
+            const uint64_t da = sdesc(a0 + (uint32_t)r * 16, TPLANE, 128);
+            mma_bf16(tmem + (uint32_t)(zo * N), da, db, idesc, (c > 0 || t > 0) ? 1u : 0u);
+          }
+        }
+        mma_commit(&empty[st]);
+        if (c >= 1 && c + 1 < nchunk) {
+          // chunk c + 1 reuses the stage of chunk c - 1 once its MMAs are done
+          if (!mbar_wait(&empty[(c - 1) & 1], (uint32_t)((c - 1) >> 1) & 1u, lim)) {
+            ok = false;
+            break;
+          }
+          load(c + 1);
+        }
+      }
+      if (!ok) {
+        atomicExch(err, 1);
+        bad = 1;
+        // let the copies already issued land before the shared memory is released
+        for (int st = 0; st < 2; st++)
+          for (; landed[st] < issued[st]; landed[st]++) mbar_wait(&full[st], (uint32_t)landed[st] & 1u, lim);
+      }
+      mma_commit(&done);  // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+  }
+  const bool fin = mbar_wait(&done, 0, 1ll << 24);
+  tc_fence_after();
+  __syncthreads();
+  if (!fin) {
+    if (tid == 0) atomicExch(err, 1);
+  } else if (!bad) {
+    // epilogue: warp w holds accumulator rows (x) 32w .. 32w + 31
+    for (int zo = 0; zo < TZ; zo++) {
+      const size_t vox = (((size_t)b * s.Y + y) * s.X + x0 + warp * 32 + lane) * s.Z + z0 + zo;
+      for (int n0 = 0; n0 < N; n0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(zo * N + n0), v);
+        if (EPI == 2) {
+          float *o = reinterpret_cast<float *>(out) + vox * N + n0;
+#pragma unroll
+          for (int q = 0; q < 16; q += 4)
+            *reinterpret_cast<float4 *>(o + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+        } else {
+          __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+          for (int q = 0; q < 16; q++) {
+            float t = v[q];
+            if (EPI == 0) t = fmaxf(t + bias[n0 + q], 0.f);
+            h[q] = __float2bfloat16_rn(t);
+          }
+          __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(out) + vox * N + n0;
+          *reinterpret_cast<int4 *>(o) = *reinterpret_cast<const int4 *>(h);
+          *reinterpret_cast<int4 *>(o + 8) = *reinterpret_cast<const int4 *>(h + 8);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_free(tmem, tmem_cols(TZ * N));
+  }
+}
+
+// K-major W[n][kpad] (k = tap * cin + ci) -> Wp[chunk][tap][half][n][8], ci = 16 chunk + 8 half + e
+__global__ void k_pack_tile_w(int cin, int n, int kpad, const __nv_bfloat16 *__restrict__ w,
+                              __nv_bfloat16 *__restrict__ wp) {
+  const long long total = (long long)((cin + 15) / 16) * 27 * 2 * n * 8;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    long long r = i;
+    const int e = (int)(r % 8);
+    r /= 8;
+    const int nn = (int)(r % n);
+    r /= n;
+    const int h = (int)(r % 2);
+    r /= 2;
+    const int t = (int)(r % 27);
+    const int c = (int)(r / 27);
+    const int ci = 16 * c + 8 * h + e;
+    wp[i] = ci < cin ? w[(size_t)nn * kpad + (size_t)t * cin + ci] : __float2bfloat16_rn(0.f);
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+}  // namespace
+
+bool conv_tile_supported(const ConvShape &s) {
+  return s.nb >= 1 && s.Y >= 1 && s.X >= TX && s.X % TX == 0 && s.Z >= TZ && s.Z % TZ == 0 && s.cin >= 8 &&
+         s.cin % 8 == 0 && s.n >= 16 && s.n % 16 == 0 && s.n <= TN_MAX && (long long)s.nb * s.Y < 65536 &&
+         encode_fn() != nullptr;
+}
+
+size_t conv_tile_wp_elems(int cin, int n) { return (size_t)((cin + 15) / 16) * 27 * 2 * n * 8; }
+
+cudaError_t conv_tile_pack(int cin, int n, int kpad, const __nv_bfloat16 *w, __nv_bfloat16 *wp, cudaStream_t st) {
+  const long long total = (long long)conv_tile_wp_elems(cin, n);
+  const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, 4096);
+  k_pack_tile_w<<<grid, 256, 0, st>>>(cin, n, kpad, w, wp);
+  return cudaGetLastError();
+}
+
+cudaError_t conv_forward_tile(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *wp, const float *bias,
+                              void *out, int epi, int sign, int *err, cudaStream_t st) {
+  if (!conv_tile_supported(s) || (epi == 0 && !bias) || epi < 0 || epi > 2 || (sign != 1 && sign != -1))
+    return cudaErrorNotSupported;
+  // activations [nb][Y][X][Z][cin] seen as (c, x, z, y, b): the box lands x-fastest
+  CUtensorMap m;
+  const cuuint64_t C2 = (cuuint64_t)s.cin * 2;
+  const cuuint64_t dims[5] = {(cuuint64_t)s.cin, (cuuint64_t)s.X, (cuuint64_t)s.Z, (cuuint64_t)s.Y,
+                              (cuuint64_t)s.nb};
+  const cuuint64_t strides[4] = {(cuuint64_t)s.Z * C2, C2, (cuuint64_t)s.X * s.Z * C2,
+                                 (cuuint64_t)s.Y * s.X * s.Z * C2};
+  const cuuint32_t box[5] = {8, TXS, TZS, 3, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  if (encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16 *>(in), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorNotSupported;
+  typedef void (*K)(const CUtensorMap, ConvShape, const __nv_bfloat16 *, const float *, void *, int *);
+  K k;
+  if (sign > 0)
+    k = epi == 0 ? k_conv_tile<1, 0> : epi == 1 ? k_conv_tile<1, 1> : k_conv_tile<1, 2>;
+  else
+    k = epi == 0 ? k_conv_tile<-1, 0> : epi == 1 ? k_conv_tile<-1, 1> : k_conv_tile<-1, 2>;
+  // one stage when the input has a single 16-channel chunk: two CTAs fit on an SM
+  const size_t smem = (s.cin > 16 ? 2 : 1) * ((size_t)TA_STAGE + b_stage_bytes(s.n));
+  cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<dim3((unsigned)(s.X / TX), (unsigned)(s.Z / TZ), (unsigned)(s.nb * s.Y)), 128, smem, st>>>(m, s, wp, bias, out,
+                                                                                              err);
+  return cudaGetLastError();
+}
+
+}  // namespace xtc

@@ -34,6 +34,7 @@ struct Layer {
   int cin_real, cin, cout, kpad, kpad_t;
   size_t off_w, off_b;  // offsets in the parameter vector
   bf16 *W = nullptr, *Wt = nullptr;
+  bf16 *Wp = nullptr;  // W packed for the tile kernel
 };
 
 struct Buf {
@@ -104,6 +105,7 @@ int pack_all(xtc_net *n) {
   for (int i = 0; i < kLayers; i++) {
     Layer &l = n->L[i];
     xtc::pack_weights(l.cin_real, l.cin, l.cout, l.kpad, l.kpad_t, n->P + l.off_w, l.W, i ? l.Wt : nullptr, n->st);
+    if (l.Wp) NCK(xtc::conv_tile_pack(l.cin, l.cout, l.kpad, l.W, l.Wp, n->st));
   }
   NCK(cudaGetLastError());
   n->packed = true;
@@ -156,6 +158,14 @@ int ensure_buffers(xtc_net *n, int nb, int Y, int X, int Z) {
 int conv(xtc_net *n, int li, const bf16 *in, int lvl, bf16 *out) {
   const Layer &l = n->L[li];
   xtc::ConvShape s{n->nb, n->Y >> lvl, n->X >> lvl, n->Z >> lvl, l.cin, l.cout, l.kpad};
+  if (l.Wp && xtc::conv_tile_supported(s)) {
+    const cudaError_t e = xtc::conv_forward_tile(s, in, l.Wp, n->P + l.off_b, out, 0, 1, n->d_err, n->st);
+    if (e != cudaErrorNotSupported) {
+      NCK(e);
+      return 0;
+    }
+    cudaGetLastError();
+  }
   NCK(xtc::conv_forward(s, in, l.W, n->P + l.off_b, out, 0, 1, n->d_err, n->st));
   return 0;
 }
@@ -312,6 +322,7 @@ int xtc_net_create(uint64_t seed, xtc_net **out) {
     Layer &l = n->L[i];
     A((void **)&l.W, (size_t)l.cout * l.kpad * 2);
     if (i) A((void **)&l.Wt, (size_t)l.cin * l.kpad_t * 2);
+    if (l.cout <= 64) A((void **)&l.Wp, xtc::conv_tile_wp_elems(l.cin, l.cout) * 2);
   }
   if (e == cudaSuccess) e = cudaMemcpy(n->P, h.data(), off * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(n->M, 0, off * 4);
@@ -335,6 +346,7 @@ void xtc_net_destroy(xtc_net *n) {
   for (int i = 0; i < kLayers; i++) {
     if (n->L[i].W) cudaFree(n->L[i].W);
     if (n->L[i].Wt) cudaFree(n->L[i].Wt);
+    if (n->L[i].Wp) cudaFree(n->L[i].Wp);
   }
   delete n;
 }

@@ -49,6 +49,36 @@ __global__ void k_avgpool(int nb, int Y, int X, int Z, int C, const __nv_bfloat1
   }
 }
 
+// the same pooling on 8-channel groups (C a multiple of 8): 16-byte loads and
+// stores, each channel summed in the same order as above
+__global__ void k_avgpool8(int nb, int Y, int X, int Z, int G, const int4 *in, int4 *out) {
+  const int Yo = Y / 2, Xo = X / 2, Zo = Z / 2;
+  const long long n = (long long)nb * Yo * Xo * Zo * G;
+  GRID_STRIDE(i, n) {
+    long long r = i;
+    const int g = (int)(r % G);
+    r /= G;
+    const int z = (int)(r % Zo);
+    r /= Zo;
+    const int x = (int)(r % Xo);
+    r /= Xo;
+    const int y = (int)(r % Yo);
+    const int b = (int)(r / Yo);
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int d = 0; d < 8; d++) {
+      const int yy = 2 * y + (d >> 2), xx = 2 * x + ((d >> 1) & 1), zz = 2 * z + (d & 1);
+      const int4 q = __ldg(in + ((((size_t)b * Y + yy) * X + xx) * Z + zz) * G + g);
+      const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&q);
+#pragma unroll
+      for (int c = 0; c < 8; c++) s[c] += __bfloat162float(h[c]);
+    }
+    __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) o[c] = __float2bfloat16_rn(s[c] * 0.125f);
+    out[i] = *reinterpret_cast<const int4 *>(o);
+  }
+}
+
 // gradient of the pooling, added into dIn (FP32 accumulation buffer)
 __global__ void k_avgpool_back(int nb, int Y, int X, int Z, int C, const float *dout, float *din) {
   const long long n = (long long)nb * Y * X * Z * C;
@@ -83,6 +113,29 @@ __global__ void k_up_concat(int nb, int Y, int X, int Z, int Ca, int Cb, const _
     const int b = (int)(r / Y);
     out[i] = c < Ca ? a[((((size_t)b * (Y / 2) + y / 2) * (X / 2) + x / 2) * (Z / 2) + z / 2) * Ca + c]
                     : skip[((((size_t)b * Y + y) * X + x) * Z + z) * Cb + (c - Ca)];
+  }
+}
+
+// the same on 8-channel groups (Ca, Cb multiples of 8): one 16-byte copy per group
+__global__ void k_up_concat8(int nb, int Y, int X, int Z, int Ga, int Gb, const int4 *a, const int4 *skip,
+                             int4 *out) {
+  const int G = Ga + Gb;
+  const long long n = (long long)nb * Y * X * Z * G;
+  GRID_STRIDE(i, n) {
+    const long long v = i / G;
+    const int g = (int)(i - v * G);
+    if (g < Ga) {
+      long long r = v;
+      const int z = (int)(r % Z);
+      r /= Z;
+      const int x = (int)(r % X);
+      r /= X;
+      const int y = (int)(r % Y);
+      const int b = (int)(r / Y);
+      out[i] = __ldg(a + ((((size_t)b * (Y / 2) + y / 2) * (X / 2) + x / 2) * (Z / 2) + z / 2) * Ga + g);
+    } else {
+      out[i] = __ldg(skip + v * Gb + (g - Ga));
+    }
   }
 }
 
@@ -151,7 +204,16 @@ __global__ void k_head(long long nv, int C, const __nv_bfloat16 *h, const float 
   double lsum = 0.0;
   GRID_STRIDE(v, nv) {
     float acc = bias[0];
-    for (int c = 0; c < C; c++) acc += __bfloat162float(h[v * C + c]) * w[c];
+    if (C % 8 == 0) {
+      for (int c0 = 0; c0 < C; c0 += 8) {
+        const int4 q = __ldg(reinterpret_cast<const int4 *>(h + v * C + c0));
+        const __nv_bfloat16 *hq = reinterpret_cast<const __nv_bfloat16 *>(&q);
+#pragma unroll
+        for (int c = 0; c < 8; c++) acc += __bfloat162float(hq[c]) * w[c0 + c];
+      }
+    } else {
+      for (int c = 0; c < C; c++) acc += __bfloat162float(h[v * C + c]) * w[c];
+    }
     const float out = base[v] + acc / scale;
     if (y) y[v] = out;
     if (target) {
@@ -251,14 +313,23 @@ void pack_input(long long nv, const float *a, const float *b, float scale, __nv_
   k_pack_input<<<blocks(nv), 256, 0, st>>>(nv, a, b, scale, out);
 }
 void avgpool(int nb, int Y, int X, int Z, int C, const __nv_bfloat16 *in, __nv_bfloat16 *out, cudaStream_t st) {
-  k_avgpool<<<blocks((long long)nb * Y * X * Z * C / 8), 256, 0, st>>>(nb, Y, X, Z, C, in, out);
+  if (C % 8 == 0)
+    k_avgpool8<<<blocks((long long)nb * Y * X * Z * C / 64), 256, 0, st>>>(
+        nb, Y, X, Z, C / 8, reinterpret_cast<const int4 *>(in), reinterpret_cast<int4 *>(out));
+  else
+    k_avgpool<<<blocks((long long)nb * Y * X * Z * C / 8), 256, 0, st>>>(nb, Y, X, Z, C, in, out);
 }
 void avgpool_back(int nb, int Y, int X, int Z, int C, const float *dout, float *din, cudaStream_t st) {
   k_avgpool_back<<<blocks((long long)nb * Y * X * Z * C), 256, 0, st>>>(nb, Y, X, Z, C, dout, din);
 }
 void up_concat(int nb, int Y, int X, int Z, int Ca, int Cb, const __nv_bfloat16 *a, const __nv_bfloat16 *skip,
                __nv_bfloat16 *out, cudaStream_t st) {
-  k_up_concat<<<blocks((long long)nb * Y * X * Z * (Ca + Cb)), 256, 0, st>>>(nb, Y, X, Z, Ca, Cb, a, skip, out);
+  if (Ca % 8 == 0 && Cb % 8 == 0)
+    k_up_concat8<<<blocks((long long)nb * Y * X * Z * (Ca + Cb) / 8), 256, 0, st>>>(
+        nb, Y, X, Z, Ca / 8, Cb / 8, reinterpret_cast<const int4 *>(a), reinterpret_cast<const int4 *>(skip),
+        reinterpret_cast<int4 *>(out));
+  else
+    k_up_concat<<<blocks((long long)nb * Y * X * Z * (Ca + Cb)), 256, 0, st>>>(nb, Y, X, Z, Ca, Cb, a, skip, out);
 }
 void up_concat_back(int nb, int Y, int X, int Z, int Ca, int Cb, const float *dout, float *da, float *dskip,
                     cudaStream_t st) {
