@@ -17,11 +17,14 @@
 // (the canonical K-major B layout of one MMA per tap) and are copied with one
 // bulk copy per stage.  One thread issues the TMA, the bulk copies and all
 // MMAs; stages are double-buffered so the copies for chunk c + 1 overlap the
-// MMAs of chunk c.  Every wait is bounded and reports through *err.
+// MMAs of chunk c, across tile boundaries too (persistent CTAs), and the
+// accumulators are double-buffered in TMEM so the epilogue of one tile
+// overlaps the next.  Every wait is bounded and reports through *err.
 //
 // Shapes: X a multiple of 128, Z even, cin a multiple of 8, cout a multiple of
-// 16 up to 64 (shared memory: 2 x (49,920 + 864 cout) bytes, one stage for
-// cin <= 16).  Other shapes use the gather kernel.
+// 16 up to 64.  Tiles are 4 z-lines high for cout <= 32 (shared memory
+// 2 x (75,008 + 864 cout) bytes), else 2 (2 x (49,920 + 864 cout)).  Other
+// shapes use the gather kernel.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -37,53 +40,82 @@ namespace xtc {
 namespace {
 
 constexpr int TX = 128, TXS = TX + 2;  // output x-voxels per tile, staged with one halo each side
-constexpr int TZ = 2, TZS = TZ + 2;    // output z-lines per tile
-constexpr int TROWS = 3 * TZS * TXS;   // staged voxels (rows) per 8-channel plane
-constexpr uint32_t TPLANE = TROWS * 16;
-constexpr uint32_t TA_STAGE = 2 * TPLANE;  // 16 channels
 constexpr int TN_MAX = 64;
-static_assert(TPLANE % 128 == 0, "TMA destinations must stay 128-byte aligned");
+
+// per tile height TZ (output z-lines): 4 for cout <= 32, else 2 (shared memory)
+template <int TZ>
+struct TileDims {
+  static constexpr int TZS = TZ + 2;                   // staged z-lines
+  static constexpr int ROWS = 3 * TZS * TXS;           // staged voxels per 8-channel plane
+  static constexpr uint32_t BOX = ROWS * 16;           // bytes one TMA box writes
+  static constexpr uint32_t PLANE = (BOX + 127) / 128 * 128;  // plane pitch: TMA destinations 128-byte aligned
+  static constexpr uint32_t A_STAGE = 2 * PLANE;       // 16 channels
+};
 
 __host__ __device__ constexpr uint32_t b_stage_bytes(int n) { return 27u * (uint32_t)n * 32u; }
 
-template <int SIGN, int EPI>
-__global__ void __launch_bounds__(128, 1)
+// Persistent: each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// Warp 4 (one thread) issues the copies and MMAs of the CTA's whole chunk
+// sequence through two shared-memory stages; the accumulators alternate
+// between two TMEM buffers, so warps 0-3 (TMEM lanes 32w .. 32w + 31) drain
+// tile i while tile i + 1 is computed.
+template <int SIGN, int EPI, int TZ>
+__global__ void __launch_bounds__(160, 1)
     k_conv_tile(const __grid_constant__ CUtensorMap tin, ConvShape s, const __nv_bfloat16 *__restrict__ wp,
                 const float *__restrict__ bias, void *out, int *err) {
+  using D = TileDims<TZ>;
+  constexpr int TZS = D::TZS;
+  constexpr uint32_t TPLANE = D::PLANE, TA_STAGE = D::A_STAGE;
   extern __shared__ __align__(1024) uint8_t sm[];
   const int N = s.n;
   const uint32_t B_STAGE = b_stage_bytes(N);
-  const int nchunk = (s.cin + 15) >> 4;
-  uint8_t *sA = sm, *sB = sm + (nchunk > 1 ? 2 : 1) * TA_STAGE;
-  __shared__ uint64_t full[2], empty[2], done;
+  uint8_t *sA = sm, *sB = sm + 2 * TA_STAGE;
+  __shared__ uint64_t full[2], empty[2], acc_full[2], acc_empty[2], done;
   __shared__ uint32_t tbase;
-  __shared__ int bad;
+  __shared__ volatile int bad;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int x0 = blockIdx.x * TX, z0 = blockIdx.y * TZ;
-  const int y = blockIdx.z % s.Y, b = blockIdx.z / s.Y;
+  const int nchunk = (s.cin + 15) >> 4;
+  const int XT = s.X / TX, ZT = s.Z / TZ;
+  const int ntiles = XT * ZT * s.nb * s.Y;
+  const int mine = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const uint32_t acc_cols = tmem_cols(2 * TZ * N);
+  const long long lim = 1ll << 24;
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 4);
+    }
     mbar_init(&done, 1);
     mbar_init_fence();
     bad = 0;
   }
-  if (warp == 0) tmem_alloc(&tbase, tmem_cols(TZ * N));
+  if (warp == 0) tmem_alloc(&tbase, acc_cols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tbase;
-  if (warp == 0) {
-    if (lane == 0) {
+  auto tile_of = [&](int tl, int &x0, int &z0, int &y, int &b) {
+    int t = (int)blockIdx.x + tl * (int)gridDim.x;
+    x0 = (t % XT) * TX;
+    t /= XT;
+    z0 = (t % ZT) * TZ;
+    t /= ZT;
+    y = t % s.Y;
+    b = t / s.Y;
+  };
+  if (warp == 4) {
+    if (lane == 0 && mine > 0) {
       const uint32_t idesc = idesc_bf16(N, 0, 0);
-      const long long lim = 1ll << 24;
+      const int Q = mine * nchunk;
       int issued[2] = {0, 0}, landed[2] = {0, 0};
-      auto load = [&](int c) {
-        const int st = c & 1;
+      auto load = [&](int q) {
+        const int st = q & 1, c = q % nchunk;
+        int x0, z0, y, b;
+        tile_of(q / nchunk, x0, z0, y, b);
         uint8_t *a = sA + st * TA_STAGE;
-        mbar_expect_tx(&full[st], TA_STAGE + B_STAGE);
+        mbar_expect_tx(&full[st], 2 * D::BOX + B_STAGE);
         // channels 16c .. 16c + 7 and 16c + 8 .. 16c + 15 (past cin: zero fill)
         tma_load_5d(a, &tin, 16 * c, x0 - 1, z0 - 1, y - 1, b, &full[st]);
         tma_load_5d(a + TPLANE, &tin, 16 * c + 8, x0 - 1, z0 - 1, y - 1, b, &full[st]);
@@ -92,85 +124,103 @@ __global__ void __launch_bounds__(128, 1)
       };
       bool ok = true;
       load(0);
-      if (nchunk > 1) load(1);
-      for (int c = 0; c < nchunk; c++) {
-        const int st = c & 1;
-        if (!mbar_wait(&full[st], (uint32_t)(c >> 1) & 1u, lim)) {
+      if (Q > 1) load(1);
+      for (int q = 0; q < Q && ok; q++) {
+        const int st = q & 1, c = q % nchunk, tl = q / nchunk, ab = tl & 1;
+        if (c == 0 && !mbar_wait(&acc_empty[ab], (uint32_t)(((tl >> 1) & 1) ^ 1), lim)) {
+          ok = false;
+          break;
+        }
+        if (!mbar_wait(&full[st], (uint32_t)(q >> 1) & 1u, lim)) {
           ok = false;
           break;
         }
         landed[st]++;
         tc_fence_after();
-        const uint32_t a0 = smem_u32(sA + st * TA_STAGE), b0 = smem_u32(sB + st * B_STAGE);
+        // descriptors advance in 16-byte units: one A row per unit, a tap's
+        // B block (N x 32 bytes) by 2N; every start stays inside the stage
+        const uint32_t acc = tmem + (uint32_t)(ab * TZ * N);
+        const uint64_t da0 = sdesc(smem_u32(sA + st * TA_STAGE) + (uint32_t)((TZS + 1) * TXS + 1) * 16, TPLANE, 128);
+        uint64_t db = sdesc(smem_u32(sB + st * B_STAGE), (uint32_t)N * 16, 128);
+        const uint64_t db_step = (uint64_t)(2 * N);
+#pragma unroll
         for (int t = 0; t < 27; t++) {
           const int dy = SIGN * (t / 9 - 1), dx = SIGN * ((t / 3) % 3 - 1), dz = SIGN * (t % 3 - 1);
           const int shift = (dy * TZS + dz) * TXS + dx;
-          const uint64_t db = sdesc(b0 + (uint32_t)t * N * 32, (uint32_t)N * 16, 128);
 #pragma unroll
-          for (int zo = 0; zo < TZ; zo++) {
-            const int r = (TZS + zo + 1) * TXS + 1 + shift;  // output line (y, z0 + zo), x = x0
-            const uint64_t da = sdesc(a0 + (uint32_t)r * 16, TPLANE, 128);
-            mma_bf16(tmem + (uint32_t)(zo * N), da, db, idesc, (c > 0 || t > 0) ? 1u : 0u);
-          }
+          for (int zo = 0; zo < TZ; zo++)
+            mma_bf16(acc + (uint32_t)(zo * N), da0 + (uint64_t)(int64_t)(shift + zo * TXS), db, idesc,
+                     (c > 0 || t > 0) ? 1u : 0u);
+          db += db_step;
         }
         mma_commit(&empty[st]);
-        if (c >= 1 && c + 1 < nchunk) {
-          // chunk c + 1 reuses the stage of chunk c - 1 once its MMAs are done
-          if (!mbar_wait(&empty[(c - 1) & 1], (uint32_t)((c - 1) >> 1) & 1u, lim)) {
+        if (c == nchunk - 1) mma_commit(&acc_full[ab]);
+        if (q >= 1 && q + 1 < Q) {
+          // chunk q + 1 reuses the stage of chunk q - 1 once its MMAs are done
+          if (!mbar_wait(&empty[(q - 1) & 1], (uint32_t)((q - 1) >> 1) & 1u, lim)) {
             ok = false;
             break;
           }
-          load(c + 1);
+          load(q + 1);
         }
       }
-      if (!ok) {
+      if (!ok || bad) {
         atomicExch(err, 1);
         bad = 1;
         // let the copies already issued land before the shared memory is released
         for (int st = 0; st < 2; st++)
           for (; landed[st] < issued[st]; landed[st]++) mbar_wait(&full[st], (uint32_t)landed[st] & 1u, lim);
       }
-      mma_commit(&done);  // arrives once every MMA issued above has completed
+      mma_commit(&done);
+      mbar_wait(&done, 0, lim);  // every MMA issued above has completed
     }
     __syncwarp();
-  }
-  const bool fin = mbar_wait(&done, 0, 1ll << 24);
-  tc_fence_after();
-  __syncthreads();
-  if (!fin) {
-    if (tid == 0) atomicExch(err, 1);
-  } else if (!bad) {
-    // epilogue: warp w holds accumulator rows (x) 32w .. 32w + 31
-    for (int zo = 0; zo < TZ; zo++) {
-      const size_t vox = (((size_t)b * s.Y + y) * s.X + x0 + warp * 32 + lane) * s.Z + z0 + zo;
-      for (int n0 = 0; n0 < N; n0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(zo * N + n0), v);
-        if (EPI == 2) {
-          float *o = reinterpret_cast<float *>(out) + vox * N + n0;
+  } else {
+    // epilogue: warp w drains accumulator rows (x) 32w .. 32w + 31
+    for (int tl = 0; tl < mine; tl++) {
+      const int ab = tl & 1;
+      if (!mbar_wait(&acc_full[ab], (uint32_t)(tl >> 1) & 1u, lim) || bad) {
+        if (lane == 0) atomicExch(err, 1);
+        bad = 1;
+        break;
+      }
+      tc_fence_after();
+      int x0, z0, y, b;
+      tile_of(tl, x0, z0, y, b);
+      for (int zo = 0; zo < TZ; zo++) {
+        const size_t vox = (((size_t)b * s.Y + y) * s.X + x0 + warp * 32 + lane) * s.Z + z0 + zo;
+        for (int n0 = 0; n0 < N; n0 += 16) {
+          float v[16];
+          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ab * TZ + zo) * N + n0), v);
+          if (EPI == 2) {
+            float *o = reinterpret_cast<float *>(out) + vox * N + n0;
 #pragma unroll
-          for (int q = 0; q < 16; q += 4)
-            *reinterpret_cast<float4 *>(o + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
-        } else {
-          __align__(16) __nv_bfloat16 h[16];
+            for (int q = 0; q < 16; q += 4)
+              *reinterpret_cast<float4 *>(o + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+          } else {
+            __align__(16) __nv_bfloat16 h[16];
 #pragma unroll
-          for (int q = 0; q < 16; q++) {
-            float t = v[q];
-            if (EPI == 0) t = fmaxf(t + bias[n0 + q], 0.f);
-            h[q] = __float2bfloat16_rn(t);
+            for (int q = 0; q < 16; q++) {
+              float t = v[q];
+              if (EPI == 0) t = fmaxf(t + bias[n0 + q], 0.f);
+              h[q] = __float2bfloat16_rn(t);
+            }
+            __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(out) + vox * N + n0;
+            *reinterpret_cast<int4 *>(o) = *reinterpret_cast<const int4 *>(h);
+            *reinterpret_cast<int4 *>(o + 8) = *reinterpret_cast<const int4 *>(h + 8);
           }
-          __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(out) + vox * N + n0;
-          *reinterpret_cast<int4 *>(o) = *reinterpret_cast<const int4 *>(h);
-          *reinterpret_cast<int4 *>(o + 8) = *reinterpret_cast<const int4 *>(h + 8);
         }
       }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[ab]);
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_free(tmem, tmem_cols(TZ * N));
+    tmem_free(tmem, acc_cols);
   }
 }
 
@@ -209,10 +259,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 }  // namespace
 
+// tile height for a shape: 4 z-lines when cout <= 32 and Z allows, else 2
+static int tile_tz(const ConvShape &s) { return (s.n <= 32 && s.Z % 4 == 0) ? 4 : 2; }
+
 bool conv_tile_supported(const ConvShape &s) {
-  return s.nb >= 1 && s.Y >= 1 && s.X >= TX && s.X % TX == 0 && s.Z >= TZ && s.Z % TZ == 0 && s.cin >= 8 &&
-         s.cin % 8 == 0 && s.n >= 16 && s.n % 16 == 0 && s.n <= TN_MAX && (long long)s.nb * s.Y < 65536 &&
-         encode_fn() != nullptr;
+  return s.nb >= 1 && s.Y >= 1 && s.X >= TX && s.X % TX == 0 && s.Z >= 2 && s.Z % 2 == 0 && s.cin >= 8 &&
+         s.cin % 8 == 0 && s.n >= 16 && s.n % 16 == 0 && s.n <= TN_MAX &&
+         (long long)(s.X / TX) * (s.Z / 2) * s.nb * s.Y < (1ll << 31) && encode_fn() != nullptr;
 }
 
 size_t conv_tile_wp_elems(int cin, int n) { return (size_t)((cin + 15) / 16) * 27 * 2 * n * 8; }
@@ -235,7 +288,8 @@ cudaError_t conv_forward_tile(const ConvShape &s, const __nv_bfloat16 *in, const
                               (cuuint64_t)s.nb};
   const cuuint64_t strides[4] = {(cuuint64_t)s.Z * C2, C2, (cuuint64_t)s.X * s.Z * C2,
                                  (cuuint64_t)s.Y * s.X * s.Z * C2};
-  const cuuint32_t box[5] = {8, TXS, TZS, 3, 1};
+  const int tz = tile_tz(s);
+  const cuuint32_t box[5] = {8, TXS, (cuuint32_t)tz + 2, 3, 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   if (encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16 *>(in), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -243,16 +297,30 @@ cudaError_t conv_forward_tile(const ConvShape &s, const __nv_bfloat16 *in, const
     return cudaErrorNotSupported;
   typedef void (*K)(const CUtensorMap, ConvShape, const __nv_bfloat16 *, const float *, void *, int *);
   K k;
-  if (sign > 0)
-    k = epi == 0 ? k_conv_tile<1, 0> : epi == 1 ? k_conv_tile<1, 1> : k_conv_tile<1, 2>;
-  else
-    k = epi == 0 ? k_conv_tile<-1, 0> : epi == 1 ? k_conv_tile<-1, 1> : k_conv_tile<-1, 2>;
-  // one stage when the input has a single 16-channel chunk: two CTAs fit on an SM
-  const size_t smem = (s.cin > 16 ? 2 : 1) * ((size_t)TA_STAGE + b_stage_bytes(s.n));
+  if (tz == 4) {
+    if (sign > 0)
+      k = epi == 0 ? k_conv_tile<1, 0, 4> : epi == 1 ? k_conv_tile<1, 1, 4> : k_conv_tile<1, 2, 4>;
+    else
+      k = epi == 0 ? k_conv_tile<-1, 0, 4> : epi == 1 ? k_conv_tile<-1, 1, 4> : k_conv_tile<-1, 2, 4>;
+  } else {
+    if (sign > 0)
+      k = epi == 0 ? k_conv_tile<1, 0, 2> : epi == 1 ? k_conv_tile<1, 1, 2> : k_conv_tile<1, 2, 2>;
+    else
+      k = epi == 0 ? k_conv_tile<-1, 0, 2> : epi == 1 ? k_conv_tile<-1, 1, 2> : k_conv_tile<-1, 2, 2>;
+  }
+  const size_t smem =
+      2 * ((size_t)(tz == 4 ? TileDims<4>::A_STAGE : TileDims<2>::A_STAGE) + b_stage_bytes(s.n));
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k<<<dim3((unsigned)(s.X / TX), (unsigned)(s.Z / TZ), (unsigned)(s.nb * s.Y)), 128, smem, st>>>(m, s, wp, bias, out,
-                                                                                              err);
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  }
+  const long long ntiles = (long long)(s.X / TX) * (s.Z / tz) * s.nb * s.Y;
+  const unsigned grid = (unsigned)std::min<long long>(ntiles, sms);  // one CTA per SM (shared memory)
+  k<<<grid, 160, smem, st>>>(m, s, wp, bias, out, err);
   return cudaGetLastError();
 }
 
