@@ -70,7 +70,7 @@ int xtc_conv3d_path(const void *in, const void *w, const float *bias, void *out,
       if ((e = cudaMalloc(&wp, need)) != cudaSuccess) return fail(e, "xtc_conv3d");
       wp_bytes = need;
     }
-    e = xtc::conv_tile_pack(cin, cout, kpad, (const __nv_bfloat16 *)w, (__nv_bfloat16 *)wp, 0);
+    e = xtc::conv_tile_pack(cin, cout, kpad, sign, (const __nv_bfloat16 *)w, (__nv_bfloat16 *)wp, 0);
     if (e == cudaSuccess)
       e = xtc::conv_forward_tile(s, (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)wp, bias, out, epi, sign,
                                  g_err, 0);

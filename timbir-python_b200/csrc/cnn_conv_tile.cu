@@ -13,9 +13,17 @@
 // 8-row core matrices 128 bytes apart, the two 8-channel halves of an MMA one
 // plane apart).  No im2col gather is ever materialised.
 //
-// Weights come pre-packed per 16-channel chunk as Wp[chunk][tap][half][n][8]
-// (the canonical K-major B layout of one MMA per tap) and are copied with one
-// bulk copy per stage.  One thread issues the TMA, the bulk copies and all
+// One MMA serves up to three output lines: staged z-line L feeds output lines
+// L - 1, L and L + 1 through the taps dz = +1, 0, -1, so with the weights of
+// those three taps stacked along N (the accumulators of consecutive output
+// lines are consecutive TMEM columns) each (L, dy, dx) is one MMA of N = up to
+// 3 cout -- half the MMAs, and half the A reads from shared memory, of one
+// MMA per (output line, tap).  The accumulators are zeroed by the epilogue
+// warps (tcgen05.st) and every MMA accumulates.
+//
+// Weights come pre-packed per 16-channel chunk as
+// Wp[chunk][dy, dx][half][dz = +1, 0, -1][n][8] (offsets as the kernel applies
+// them, i.e. mirrored for sign -1) and are copied with one bulk copy per stage.  One thread issues the TMA, the bulk copies and all
 // MMAs; stages are double-buffered so the copies for chunk c + 1 overlap the
 // MMAs of chunk c, across tile boundaries too (persistent CTAs), and the
 // accumulators are double-buffered in TMEM so the epilogue of one tile
@@ -59,7 +67,7 @@ __host__ __device__ constexpr uint32_t b_stage_bytes(int n) { return 27u * (uint
 // sequence through two shared-memory stages; the accumulators alternate
 // between two TMEM buffers, so warps 0-3 (TMEM lanes 32w .. 32w + 31) drain
 // tile i while tile i + 1 is computed.
-template <int SIGN, int EPI, int TZ>
+template <int EPI, int TZ>
 __global__ void __launch_bounds__(160, 1)
     k_conv_tile(const __grid_constant__ CUtensorMap tin, ConvShape s, const __nv_bfloat16 *__restrict__ wp,
                 const float *__restrict__ bias, void *out, int *err) {
@@ -96,6 +104,13 @@ __global__ void __launch_bounds__(160, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tbase;
+  if (warp < 4) {  // both accumulator buffers start at zero
+    for (int col = 0; col < 2 * TZ * N; col += 16) tmem_st16_zero(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col);
+    tmem_st_wait();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
   auto tile_of = [&](int tl, int &x0, int &z0, int &y, int &b) {
     int t = (int)blockIdx.x + tl * (int)gridDim.x;
     x0 = (t % XT) * TX;
@@ -107,7 +122,7 @@ __global__ void __launch_bounds__(160, 1)
   };
   if (warp == 4) {
     if (lane == 0 && mine > 0) {
-      const uint32_t idesc = idesc_bf16(N, 0, 0);
+      const uint32_t idesc[3] = {idesc_bf16(N, 0, 0), idesc_bf16(2 * N, 0, 0), idesc_bf16(3 * N, 0, 0)};
       const int Q = mine * nchunk;
       int issued[2] = {0, 0}, landed[2] = {0, 0};
       auto load = [&](int q) {
@@ -137,21 +152,24 @@ __global__ void __launch_bounds__(160, 1)
         }
         landed[st]++;
         tc_fence_after();
-        // descriptors advance in 16-byte units: one A row per unit, a tap's
-        // B block (N x 32 bytes) by 2N; every start stays inside the stage
+        // descriptors advance in 16-byte units: one A row per unit; a (dy, dx)
+        // B block (2 halves x 3 dz x N rows x 16 bytes) by 6N, one dz block by N
         const uint32_t acc = tmem + (uint32_t)(ab * TZ * N);
         const uint64_t da0 = sdesc(smem_u32(sA + st * TA_STAGE) + (uint32_t)((TZS + 1) * TXS + 1) * 16, TPLANE, 128);
-        uint64_t db = sdesc(smem_u32(sB + st * B_STAGE), (uint32_t)N * 16, 128);
-        const uint64_t db_step = (uint64_t)(2 * N);
+        uint64_t db = sdesc(smem_u32(sB + st * B_STAGE), (uint32_t)N * 48, 128);
 #pragma unroll
-        for (int t = 0; t < 27; t++) {
-          const int dy = SIGN * (t / 9 - 1), dx = SIGN * ((t / 3) % 3 - 1), dz = SIGN * (t % 3 - 1);
-          const int shift = (dy * TZS + dz) * TXS + dx;
+        for (int g = 0; g < 9; g++) {
+          const int dy = g / 3 - 1, dx = g % 3 - 1;
 #pragma unroll
-          for (int zo = 0; zo < TZ; zo++)
-            mma_bf16(acc + (uint32_t)(zo * N), da0 + (uint64_t)(int64_t)(shift + zo * TXS), db, idesc,
-                     (c > 0 || t > 0) ? 1u : 0u);
-          db += db_step;
+          for (int zl = 0; zl < TZS; zl++) {
+            // staged line zl (z = z0 - 1 + zl) feeds output lines zl - 2 .. zl
+            // (relative to z0) through dz = +1, 0, -1; keep those inside the tile
+            const int zf = zl - 2 < 0 ? 0 : zl - 2, zt = zl > TZ - 1 ? TZ - 1 : zl;
+            const int cnt = zt - zf + 1, blk = zf - (zl - 2);
+            mma_bf16(acc + (uint32_t)(zf * N), da0 + (uint64_t)(int64_t)((dy * TZS + zl - 1) * TXS + dx),
+                     db + (uint64_t)(blk * N), idesc[cnt - 1], 1u);
+          }
+          db += (uint64_t)(6 * N);
         }
         mma_commit(&empty[st]);
         if (c == nchunk - 1) mma_commit(&acc_full[ab]);
@@ -211,6 +229,10 @@ __global__ void __launch_bounds__(160, 1)
           }
         }
       }
+      // the buffer starts the CTA's next tile at zero
+      for (int col = 0; col < TZ * N; col += 16)
+        tmem_st16_zero(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(ab * TZ * N + col));
+      tmem_st_wait();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[ab]);
@@ -224,8 +246,10 @@ __global__ void __launch_bounds__(160, 1)
   }
 }
 
-// K-major W[n][kpad] (k = tap * cin + ci) -> Wp[chunk][tap][half][n][8], ci = 16 chunk + 8 half + e
-__global__ void k_pack_tile_w(int cin, int n, int kpad, const __nv_bfloat16 *__restrict__ w,
+// K-major W[n][kpad] (k = tap * cin + ci, tap = (dy+1)*9 + (dx+1)*3 + (dz+1))
+// -> Wp[chunk][(ey+1)*3 + (ex+1)][half][dzi][n][8], ci = 16 chunk + 8 half + e,
+// effective offsets (ey, ex, ez = 1 - dzi) = sign x (dy, dx, dz)
+__global__ void k_pack_tile_w(int cin, int n, int kpad, int sign, const __nv_bfloat16 *__restrict__ w,
                               __nv_bfloat16 *__restrict__ wp) {
   const long long total = (long long)((cin + 15) / 16) * 27 * 2 * n * 8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
@@ -235,11 +259,15 @@ __global__ void k_pack_tile_w(int cin, int n, int kpad, const __nv_bfloat16 *__r
     r /= 8;
     const int nn = (int)(r % n);
     r /= n;
+    const int dzi = (int)(r % 3);
+    r /= 3;
     const int h = (int)(r % 2);
     r /= 2;
-    const int t = (int)(r % 27);
-    const int c = (int)(r / 27);
+    const int g = (int)(r % 9);
+    const int c = (int)(r / 9);
     const int ci = 16 * c + 8 * h + e;
+    const int dy = sign * (g / 3 - 1), dx = sign * (g % 3 - 1), dz = sign * (1 - dzi);
+    const int t = (dy + 1) * 9 + (dx + 1) * 3 + (dz + 1);
     wp[i] = ci < cin ? w[(size_t)nn * kpad + (size_t)t * cin + ci] : __float2bfloat16_rn(0.f);
   }
 }
@@ -270,10 +298,11 @@ bool conv_tile_supported(const ConvShape &s) {
 
 size_t conv_tile_wp_elems(int cin, int n) { return (size_t)((cin + 15) / 16) * 27 * 2 * n * 8; }
 
-cudaError_t conv_tile_pack(int cin, int n, int kpad, const __nv_bfloat16 *w, __nv_bfloat16 *wp, cudaStream_t st) {
+cudaError_t conv_tile_pack(int cin, int n, int kpad, int sign, const __nv_bfloat16 *w, __nv_bfloat16 *wp,
+                           cudaStream_t st) {
   const long long total = (long long)conv_tile_wp_elems(cin, n);
   const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, 4096);
-  k_pack_tile_w<<<grid, 256, 0, st>>>(cin, n, kpad, w, wp);
+  k_pack_tile_w<<<grid, 256, 0, st>>>(cin, n, kpad, sign, w, wp);
   return cudaGetLastError();
 }
 
@@ -297,17 +326,11 @@ cudaError_t conv_forward_tile(const ConvShape &s, const __nv_bfloat16 *in, const
     return cudaErrorNotSupported;
   typedef void (*K)(const CUtensorMap, ConvShape, const __nv_bfloat16 *, const float *, void *, int *);
   K k;
-  if (tz == 4) {
-    if (sign > 0)
-      k = epi == 0 ? k_conv_tile<1, 0, 4> : epi == 1 ? k_conv_tile<1, 1, 4> : k_conv_tile<1, 2, 4>;
-    else
-      k = epi == 0 ? k_conv_tile<-1, 0, 4> : epi == 1 ? k_conv_tile<-1, 1, 4> : k_conv_tile<-1, 2, 4>;
-  } else {
-    if (sign > 0)
-      k = epi == 0 ? k_conv_tile<1, 0, 2> : epi == 1 ? k_conv_tile<1, 1, 2> : k_conv_tile<1, 2, 2>;
-    else
-      k = epi == 0 ? k_conv_tile<-1, 0, 2> : epi == 1 ? k_conv_tile<-1, 1, 2> : k_conv_tile<-1, 2, 2>;
-  }
+  // the sign lives in the packed weights
+  if (tz == 4)
+    k = epi == 0 ? k_conv_tile<0, 4> : epi == 1 ? k_conv_tile<1, 4> : k_conv_tile<2, 4>;
+  else
+    k = epi == 0 ? k_conv_tile<0, 2> : epi == 1 ? k_conv_tile<1, 2> : k_conv_tile<2, 2>;
   const size_t smem =
       2 * ((size_t)(tz == 4 ? TileDims<4>::A_STAGE : TileDims<2>::A_STAGE) + b_stage_bytes(s.n));
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -105,7 +105,7 @@ int pack_all(xtc_net *n) {
   for (int i = 0; i < kLayers; i++) {
     Layer &l = n->L[i];
     xtc::pack_weights(l.cin_real, l.cin, l.cout, l.kpad, l.kpad_t, n->P + l.off_w, l.W, i ? l.Wt : nullptr, n->st);
-    if (l.Wp) NCK(xtc::conv_tile_pack(l.cin, l.cout, l.kpad, l.W, l.Wp, n->st));
+    if (l.Wp) NCK(xtc::conv_tile_pack(l.cin, l.cout, l.kpad, 1, l.W, l.Wp, n->st));
   }
   NCK(cudaGetLastError());
   n->packed = true;

@@ -135,6 +135,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// zero 16 consecutive FP32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_st16_zero(uint32_t taddr) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+      "%1};" ::"r"(taddr),
+      "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // TMEM columns to allocate for N accumulator columns (power of two, >= 32)
 __host__ __device__ constexpr uint32_t tmem_cols(int n) {
   return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : 256u;

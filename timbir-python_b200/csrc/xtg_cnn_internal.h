@@ -19,7 +19,8 @@ cudaError_t conv_forward(const ConvShape &s, const __nv_bfloat16 *in, const __nv
 // n <= 64; weights pre-packed by conv_tile_pack into conv_tile_wp_elems values
 bool conv_tile_supported(const ConvShape &s);
 size_t conv_tile_wp_elems(int cin, int n);
-cudaError_t conv_tile_pack(int cin, int n, int kpad, const __nv_bfloat16 *w, __nv_bfloat16 *wp, cudaStream_t st);
+cudaError_t conv_tile_pack(int cin, int n, int kpad, int sign, const __nv_bfloat16 *w, __nv_bfloat16 *wp,
+                           cudaStream_t st);
 cudaError_t conv_forward_tile(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *wp, const float *bias,
                               void *out, int epi, int sign, int *err, cudaStream_t st);
 cudaError_t conv_wgrad(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, float *dw, int *err,
