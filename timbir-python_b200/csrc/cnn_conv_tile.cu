@@ -3,15 +3,14 @@
 //
 // The gather kernel in cnn_conv.cu builds every A row (voxel x 64 K values)
 // with per-thread loads: each input voxel is fetched 27 times.  Here a CTA
-// owns an output tile of 128 x-voxels x TZ z-lines of one y-row; TMA stages
-// the tile's input halo (130 x (TZ + 2) x 3 voxels, 16 channels per stage,
-// zero filled outside the volume) in shared memory once, laid out as two
-// 8-channel planes, x fastest:  row r = (y' * TZS + z') * TXS + x'.  In that
-// layout the A operand of tap (dy, dx, dz) for output line z is the run of 128
-// rows starting at r0(z) + (dy * TZS + dz) * TXS + dx -- one shared-memory
-// descriptor with a shifted start address (K-major, no swizzle: 16-byte rows,
-// 8-row core matrices 128 bytes apart, the two 8-channel halves of an MMA one
-// plane apart).  No im2col gather is ever materialised.
+// owns an output tile of 128 x-voxels x TZ z-lines of one y-row; one TMA box
+// per 16-channel chunk stages the tile's input halo (130 x (TZ + 2) x 3
+// voxels, zero filled outside the volume) in shared memory once, one 32-byte
+// row per voxel (16 channels, the 32-byte swizzle), x fastest:
+// row r = (y' * TZS + z') * TXS + x'.  In that layout the A operand of tap
+// (dy, dx, dz) for output line z is the run of 128 rows starting at
+// r0(z) + (dy * TZS + dz) * TXS + dx -- one shared-memory descriptor with a
+// shifted start address.  No im2col gather is ever materialised.
 //
 // One MMA serves up to three output lines: staged z-line L feeds output lines
 // L - 1, L and L + 1 through the taps dz = +1, 0, -1, so with the weights of
@@ -31,7 +30,7 @@
 //
 // Shapes: X a multiple of 128, Z even, cin a multiple of 8, cout a multiple of
 // 16 up to 64.  Tiles are 4 z-lines high for cout <= 32 (shared memory
-// 2 x (75,008 + 864 cout) bytes), else 2 (2 x (49,920 + 864 cout)).  Other
+// 2 x (75,776 + 864 cout) bytes), else 2 (2 x (50,176 + 864 cout)).  Other
 // shapes use the gather kernel.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -54,11 +53,20 @@ constexpr int TN_MAX = 64;
 template <int TZ>
 struct TileDims {
   static constexpr int TZS = TZ + 2;                   // staged z-lines
-  static constexpr int ROWS = 3 * TZS * TXS;           // staged voxels per 8-channel plane
-  static constexpr uint32_t BOX = ROWS * 16;           // bytes one TMA box writes
-  static constexpr uint32_t PLANE = (BOX + 127) / 128 * 128;  // plane pitch: TMA destinations 128-byte aligned
-  static constexpr uint32_t A_STAGE = 2 * PLANE;       // 16 channels
+  static constexpr int ROWS = 3 * TZS * TXS;           // staged voxels, one 32-byte row (16 channels) each
+  static constexpr uint32_t BOX = ROWS * 32;           // bytes one TMA box writes
+  static constexpr uint32_t A_STAGE = (BOX + 1023) / 1024 * 1024;  // stages stay aligned to the swizzle atom
 };
+
+// K-major operand with 32-byte rows in the 32-byte swizzle (16-byte chunk
+// index XOR address bit 7, as TMA's SWIZZLE_32B writes it): the two 8-element
+// K halves of a row are one 16-byte unit apart, 8-row groups 256 bytes apart.
+// The swizzle is a function of the absolute shared-memory address, so a
+// descriptor may start at any row.
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(256 >> 4) << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)6 << 61);
+}
 
 __host__ __device__ constexpr uint32_t b_stage_bytes(int n) { return 27u * (uint32_t)n * 32u; }
 
@@ -73,7 +81,7 @@ __global__ void __launch_bounds__(160, 1)
                 const float *__restrict__ bias, void *out, int *err) {
   using D = TileDims<TZ>;
   constexpr int TZS = D::TZS;
-  constexpr uint32_t TPLANE = D::PLANE, TA_STAGE = D::A_STAGE;
+  constexpr uint32_t TA_STAGE = D::A_STAGE;
   extern __shared__ __align__(1024) uint8_t sm[];
   const int N = s.n;
   const uint32_t B_STAGE = b_stage_bytes(N);
@@ -130,10 +138,9 @@ __global__ void __launch_bounds__(160, 1)
         int x0, z0, y, b;
         tile_of(q / nchunk, x0, z0, y, b);
         uint8_t *a = sA + st * TA_STAGE;
-        mbar_expect_tx(&full[st], 2 * D::BOX + B_STAGE);
-        // channels 16c .. 16c + 7 and 16c + 8 .. 16c + 15 (past cin: zero fill)
+        mbar_expect_tx(&full[st], D::BOX + B_STAGE);
+        // channels 16c .. 16c + 15 (past cin: zero fill)
         tma_load_5d(a, &tin, 16 * c, x0 - 1, z0 - 1, y - 1, b, &full[st]);
-        tma_load_5d(a + TPLANE, &tin, 16 * c + 8, x0 - 1, z0 - 1, y - 1, b, &full[st]);
         bulk_load(sB + st * B_STAGE, wp + (size_t)c * (B_STAGE / 2), B_STAGE, &full[st]);
         issued[st]++;
       };
@@ -152,10 +159,10 @@ __global__ void __launch_bounds__(160, 1)
         }
         landed[st]++;
         tc_fence_after();
-        // descriptors advance in 16-byte units: one A row per unit; a (dy, dx)
+        // descriptors advance in 16-byte units: an A row by 2; a (dy, dx)
         // B block (2 halves x 3 dz x N rows x 16 bytes) by 6N, one dz block by N
         const uint32_t acc = tmem + (uint32_t)(ab * TZ * N);
-        const uint64_t da0 = sdesc(smem_u32(sA + st * TA_STAGE) + (uint32_t)((TZS + 1) * TXS + 1) * 16, TPLANE, 128);
+        const uint64_t da0 = sdesc_sw32(smem_u32(sA + st * TA_STAGE) + (uint32_t)((TZS + 1) * TXS + 1) * 32);
         uint64_t db = sdesc(smem_u32(sB + st * B_STAGE), (uint32_t)N * 48, 128);
 #pragma unroll
         for (int g = 0; g < 9; g++) {
@@ -166,7 +173,7 @@ __global__ void __launch_bounds__(160, 1)
             // (relative to z0) through dz = +1, 0, -1; keep those inside the tile
             const int zf = zl - 2 < 0 ? 0 : zl - 2, zt = zl > TZ - 1 ? TZ - 1 : zl;
             const int cnt = zt - zf + 1, blk = zf - (zl - 2);
-            mma_bf16(acc + (uint32_t)(zf * N), da0 + (uint64_t)(int64_t)((dy * TZS + zl - 1) * TXS + dx),
+            mma_bf16(acc + (uint32_t)(zf * N), da0 + (uint64_t)(int64_t)(2 * ((dy * TZS + zl - 1) * TXS + dx)),
                      db + (uint64_t)(blk * N), idesc[cnt - 1], 1u);
           }
           db += (uint64_t)(6 * N);
@@ -318,10 +325,10 @@ cudaError_t conv_forward_tile(const ConvShape &s, const __nv_bfloat16 *in, const
   const cuuint64_t strides[4] = {(cuuint64_t)s.Z * C2, C2, (cuuint64_t)s.X * s.Z * C2,
                                  (cuuint64_t)s.Y * s.X * s.Z * C2};
   const int tz = tile_tz(s);
-  const cuuint32_t box[5] = {8, TXS, (cuuint32_t)tz + 2, 3, 1};
+  const cuuint32_t box[5] = {16, TXS, (cuuint32_t)tz + 2, 3, 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   if (encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16 *>(in), dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return cudaErrorNotSupported;
   typedef void (*K)(const CUtensorMap, ConvShape, const __nv_bfloat16 *, const float *, void *, int *);
