@@ -296,6 +296,111 @@ __global__ void __launch_bounds__(CONV_THREADS) k_wgrad_tc(ConvShape s, const __
   }
 }
 
+// The network's first layer: two input channels (the FBP image and the start
+// image, FP32 [nb][Y][X][Z], times scale), so K = 27 taps x 2 = 54, padded to
+// 64: one MMA stage whose A rows are gathered straight from the FP32 volumes
+// (the input packing fused into the convolution).  w64: [n][64] BF16,
+// k = 2 tap + channel.  Output: ReLU(acc + bias) in BF16 [voxel][n].
+__global__ void __launch_bounds__(CONV_THREADS) k_conv_first(int nb, int Y, int X, int Z, const float *__restrict__ fa,
+                                                             const float *__restrict__ fb, float scale,
+                                                             const __nv_bfloat16 *__restrict__ w64,
+                                                             const float *__restrict__ bias, int N,
+                                                             __nv_bfloat16 *__restrict__ out, int *err) {
+  extern __shared__ __align__(128) uint8_t sm[];
+  uint8_t *sA = sm;                 // [8][128][16 B]
+  uint8_t *sB = sm + 128 * 64 * 2;  // [8][N][16 B]
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tbase;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const long long M = (long long)nb * Y * X * Z;
+  const long long mv = (long long)blockIdx.x * 128 + tid;
+  const bool mval = mv < M;
+  int b = 0, yy = 0, xx = 0, zz = 0;
+  if (mval) {
+    long long r = mv;
+    zz = (int)(r % Z);
+    r /= Z;
+    xx = (int)(r % X);
+    r /= X;
+    yy = (int)(r % Y);
+    b = (int)(r / Y);
+  }
+  if (tid == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+  }
+  if (warp == 0) tmem_alloc(&tbase, tmem_cols(N));
+  // A: this thread's voxel, K = (tap, channel)
+  __align__(16) __nv_bfloat16 row[64];
+#pragma unroll
+  for (int t = 0; t < 27; t++) {
+    int dy, dx, dz;
+    tap_offset(t, dy, dx, dz);
+    const int y2 = yy + dy, x2 = xx + dx, z2 = zz + dz;
+    float va = 0.f, vb = 0.f;
+    if (mval && y2 >= 0 && y2 < Y && x2 >= 0 && x2 < X && z2 >= 0 && z2 < Z) {
+      const size_t o = (((size_t)b * Y + y2) * X + x2) * Z + z2;
+      va = __ldg(fa + o) * scale;
+      vb = __ldg(fb + o) * scale;
+    }
+    row[2 * t] = __float2bfloat16_rn(va);
+    row[2 * t + 1] = __float2bfloat16_rn(vb);
+  }
+#pragma unroll
+  for (int k = 54; k < 64; k++) row[k] = __float2bfloat16_rn(0.f);
+#pragma unroll
+  for (int c = 0; c < 8; c++)
+    *reinterpret_cast<int4 *>(sA + c * (128 * 16) + tid * 16) = *reinterpret_cast<const int4 *>(row + 8 * c);
+  for (int i = tid; i < N * 8; i += CONV_THREADS) {
+    const int c = i / N, n = i - c * N;
+    *reinterpret_cast<int4 *>(sB + c * (N * 16) + n * 16) =
+        __ldg(reinterpret_cast<const int4 *>(w64 + (size_t)n * 64 + c * 8));
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tbase;
+  if (tid == 0) {
+    const uint32_t idesc = idesc_bf16(N, 0, 0), a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+    for (int ks = 0; ks < 4; ks++)
+      mma_bf16(tmem, sdesc(a0 + ks * 2 * 128 * 16, 128 * 16, 128), sdesc(b0 + ks * 2 * N * 16, N * 16, 128), idesc,
+               ks > 0 ? 1u : 0u);
+    mma_commit(&mbar);
+  }
+  const bool ok = wait_stage(&mbar, 0, err);
+  tc_fence_after();
+  if (ok) {
+    for (int n0 = 0; n0 < N; n0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)n0, v);
+      if (!mval) continue;
+      __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) h[q] = __float2bfloat16_rn(fmaxf(v[q] + bias[n0 + q], 0.f));
+      __nv_bfloat16 *o = out + (size_t)mv * N + n0;
+      *reinterpret_cast<int4 *>(o) = *reinterpret_cast<const int4 *>(h);
+      *reinterpret_cast<int4 *>(o + 8) = *reinterpret_cast<const int4 *>(h + 8);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_free(tmem, tmem_cols(N));
+  }
+}
+
+// [n][kpad] with k = tap * cin + ci (ci < 2 real) -> [n][64] with k = 2 tap + ci
+__global__ void k_pack_first(int n, int cin, int kpad, const __nv_bfloat16 *__restrict__ w,
+                             __nv_bfloat16 *__restrict__ w64) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * 64) return;
+  const int nn = i / 64, k = i % 64;
+  w64[i] = k < 54 ? w[(size_t)nn * kpad + (k / 2) * cin + (k % 2)] : __float2bfloat16_rn(0.f);
+}
+
 // Dynamic shared memory per CTA: the two operand stages, raised where needed
 // so that no more CTAs fit on an SM (228 KB) than its 512 TMEM columns hold.
 static size_t conv_smem(int n) {
@@ -338,6 +443,33 @@ cudaError_t conv_wgrad(const ConvShape &s, const __nv_bfloat16 *in, const __nv_b
   cudaError_t e = cudaFuncSetAttribute((const void *)k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k_wgrad_tc<<<dim3((unsigned)mt, (unsigned)splits), CONV_THREADS, smem, st>>>(s, in, dout, dw, (int)kchunk, err);
+  return cudaGetLastError();
+}
+
+}  // namespace xtc
+
+namespace xtc {
+
+cudaError_t conv_first_pack(int n, int cin, int kpad, const __nv_bfloat16 *w, __nv_bfloat16 *w64, cudaStream_t st) {
+  if (cin < 2) return cudaErrorInvalidValue;
+  k_pack_first<<<(n * 64 + 255) / 256, 256, 0, st>>>(n, cin, kpad, w, w64);
+  return cudaGetLastError();
+}
+
+cudaError_t conv_first(int nb, int Y, int X, int Z, const float *a, const float *b, float scale,
+                       const __nv_bfloat16 *w64, const float *bias, int n, __nv_bfloat16 *out, int *err,
+                       cudaStream_t st) {
+  if (n % 16 || n < 16 || n > 256) return cudaErrorInvalidValue;
+  const long long M = (long long)nb * Y * X * Z;
+  size_t smem = (size_t)128 * 64 * 2 + (size_t)n * 64 * 2;
+  // no more CTAs on an SM than its 512 TMEM columns hold
+  const size_t fit = 512 / tmem_cols(n), floor_bytes = 228 * 1024 / (fit + 1) + 1024;
+  if (smem < floor_bytes) smem = floor_bytes;
+  cudaError_t e =
+      cudaFuncSetAttribute((const void *)k_conv_first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_conv_first<<<(unsigned)((M + 127) / 128), CONV_THREADS, smem, st>>>(nb, Y, X, Z, a, b, scale, w64, bias, n, out,
+                                                                         err);
   return cudaGetLastError();
 }
 

@@ -34,7 +34,8 @@ struct Layer {
   int cin_real, cin, cout, kpad, kpad_t;
   size_t off_w, off_b;  // offsets in the parameter vector
   bf16 *W = nullptr, *Wt = nullptr;
-  bf16 *Wp = nullptr;  // W packed for the tile kernel
+  bf16 *Wp = nullptr;   // W packed for the tile kernel
+  bf16 *W64 = nullptr;  // the first layer's W as [cout][64], k = 2 tap + channel
 };
 
 struct Buf {
@@ -106,6 +107,7 @@ int pack_all(xtc_net *n) {
     Layer &l = n->L[i];
     xtc::pack_weights(l.cin_real, l.cin, l.cout, l.kpad, l.kpad_t, n->P + l.off_w, l.W, i ? l.Wt : nullptr, n->st);
     if (l.Wp) NCK(xtc::conv_tile_pack(l.cin, l.cout, l.kpad, 1, l.W, l.Wp, n->st));
+    if (l.W64) NCK(xtc::conv_first_pack(l.cout, l.cin, l.kpad, l.W, l.W64, n->st));
   }
   NCK(cudaGetLastError());
   n->packed = true;
@@ -176,9 +178,14 @@ int forward(xtc_net *n, const float *fbp, const float *icd, float *out, const fl
   cudaStream_t st = n->st;
   bf16 *A[kLayers];
   for (int i = 0; i < kLayers; i++) A[i] = n->a[i].as<bf16>();
-  xtc::pack_input(v0, fbp, icd, kScale, n->in0.as<bf16>(), st);
   int rc;
-  if ((rc = conv(n, 0, n->in0.as<bf16>(), 0, A[0]))) return rc;
+  if (target) {  // training keeps the packed input for the first layer's weight gradient
+    xtc::pack_input(v0, fbp, icd, kScale, n->in0.as<bf16>(), st);
+    if ((rc = conv(n, 0, n->in0.as<bf16>(), 0, A[0]))) return rc;
+  } else {
+    NCK(xtc::conv_first(nb, Y, X, Z, fbp, icd, kScale, n->L[0].W64, n->P + n->L[0].off_b, n->L[0].cout, A[0],
+                        n->d_err, st));
+  }
   if ((rc = conv(n, 1, A[0], 0, A[1]))) return rc;
   xtc::avgpool(nb, Y, X, Z, 32, A[1], n->p0.as<bf16>(), st);
   if ((rc = conv(n, 2, n->p0.as<bf16>(), 1, A[2]))) return rc;
@@ -323,6 +330,7 @@ int xtc_net_create(uint64_t seed, xtc_net **out) {
     A((void **)&l.W, (size_t)l.cout * l.kpad * 2);
     if (i) A((void **)&l.Wt, (size_t)l.cin * l.kpad_t * 2);
     if (l.cout <= 64) A((void **)&l.Wp, xtc::conv_tile_wp_elems(l.cin, l.cout) * 2);
+    if (i == 0) A((void **)&l.W64, (size_t)l.cout * 64 * 2);
   }
   if (e == cudaSuccess) e = cudaMemcpy(n->P, h.data(), off * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(n->M, 0, off * 4);
@@ -347,6 +355,7 @@ void xtc_net_destroy(xtc_net *n) {
     if (n->L[i].W) cudaFree(n->L[i].W);
     if (n->L[i].Wt) cudaFree(n->L[i].Wt);
     if (n->L[i].Wp) cudaFree(n->L[i].Wp);
+    if (n->L[i].W64) cudaFree(n->L[i].W64);
   }
   delete n;
 }

@@ -116,25 +116,22 @@ __global__ void k_up_concat(int nb, int Y, int X, int Z, int Ca, int Cb, const _
   }
 }
 
-// the same on 8-channel groups (Ca, Cb multiples of 8): one 16-byte copy per group
-__global__ void k_up_concat8(int nb, int Y, int X, int Z, int Ga, int Gb, const int4 *a, const int4 *skip,
-                             int4 *out) {
-  const int G = Ga + Gb;
-  const long long n = (long long)nb * Y * X * Z * G;
-  GRID_STRIDE(i, n) {
-    const long long v = i / G;
-    const int g = (int)(i - v * G);
+// the same on 8-channel groups (Ca, Cb multiples of 8): one 16-byte copy per
+// group, consecutive threads on consecutive output groups; GA, GB fixed at
+// compile time (0: taken from the arguments) and 32-bit indices (n < 2^31)
+template <int GA, int GB>
+__global__ void k_up_concat8(int nb, int Y, int X, int Z, int ga, int gb, const int4 *__restrict__ a,
+                             const int4 *__restrict__ skip, int4 *__restrict__ out) {
+  const unsigned Ga = GA ? GA : ga, Gb = GB ? GB : gb, G = Ga + Gb;
+  const unsigned n = (unsigned)nb * Y * X * Z * G;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned v = i / G, g = i - v * G;
     if (g < Ga) {
-      long long r = v;
-      const int z = (int)(r % Z);
-      r /= Z;
-      const int x = (int)(r % X);
-      r /= X;
-      const int y = (int)(r % Y);
-      const int b = (int)(r / Y);
-      out[i] = __ldg(a + ((((size_t)b * (Y / 2) + y / 2) * (X / 2) + x / 2) * (Z / 2) + z / 2) * Ga + g);
+      const unsigned z = v % Z, r1 = v / Z, x = r1 % X, r2 = r1 / X;  // r2 = b * Y + y
+      const unsigned cv = ((r2 >> 1) * (X >> 1) + (x >> 1)) * (Z >> 1) + (z >> 1);  // Y even: b*Y/2 + y/2
+      out[i] = __ldg(a + (size_t)cv * Ga + g);
     } else {
-      out[i] = __ldg(skip + v * Gb + (g - Ga));
+      out[i] = __ldg(skip + (size_t)v * Gb + (g - Ga));
     }
   }
 }
@@ -324,11 +321,16 @@ void avgpool_back(int nb, int Y, int X, int Z, int C, const float *dout, float *
 }
 void up_concat(int nb, int Y, int X, int Z, int Ca, int Cb, const __nv_bfloat16 *a, const __nv_bfloat16 *skip,
                __nv_bfloat16 *out, cudaStream_t st) {
-  if (Ca % 8 == 0 && Cb % 8 == 0)
-    k_up_concat8<<<blocks((long long)nb * Y * X * Z * (Ca + Cb) / 8), 256, 0, st>>>(
-        nb, Y, X, Z, Ca / 8, Cb / 8, reinterpret_cast<const int4 *>(a), reinterpret_cast<const int4 *>(skip),
-        reinterpret_cast<int4 *>(out));
-  else
+  const long long n8 = (long long)nb * Y * X * Z * (Ca + Cb) / 8;
+  if (Ca % 8 == 0 && Cb % 8 == 0 && Y % 2 == 0 && n8 < (1ll << 31)) {
+    const int ga = Ca / 8, gb = Cb / 8;
+    auto k = (ga == 6 && gb == 4)   ? k_up_concat8<6, 4>
+             : (ga == 8 && gb == 6)  ? k_up_concat8<8, 6>
+             : (ga == 12 && gb == 8) ? k_up_concat8<12, 8>
+                                     : k_up_concat8<0, 0>;
+    k<<<blocks(n8), 256, 0, st>>>(nb, Y, X, Z, ga, gb, reinterpret_cast<const int4 *>(a),
+                                  reinterpret_cast<const int4 *>(skip), reinterpret_cast<int4 *>(out));
+  } else
     k_up_concat<<<blocks((long long)nb * Y * X * Z * (Ca + Cb)), 256, 0, st>>>(nb, Y, X, Z, Ca, Cb, a, skip, out);
 }
 void up_concat_back(int nb, int Y, int X, int Z, int Ca, int Cb, const float *dout, float *da, float *dskip,

@@ -15,6 +15,11 @@ struct ConvShape {
 
 cudaError_t conv_forward(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
                          void *out, int epi, int sign, int *err, cudaStream_t st);
+// the first layer (2 FP32 input channels, the input packing fused in): w64 [n][64], k = 2 tap + channel
+cudaError_t conv_first_pack(int n, int cin, int kpad, const __nv_bfloat16 *w, __nv_bfloat16 *w64, cudaStream_t st);
+cudaError_t conv_first(int nb, int Y, int X, int Z, const float *a, const float *b, float scale,
+                       const __nv_bfloat16 *w64, const float *bias, int n, __nv_bfloat16 *out, int *err,
+                       cudaStream_t st);
 // the TMA-staged tile kernel (cnn_conv_tile.cu): X a multiple of 128, Z even,
 // n <= 64; weights pre-packed by conv_tile_pack into conv_tile_wp_elems values
 bool conv_tile_supported(const ConvShape &s);
