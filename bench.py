@@ -262,12 +262,11 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     if learned and os.path.exists(WEIGHTS) and all(d % 8 == 0 for d in (ctx.N_x, ctx.N_y, ctx.N_z)):
         net = xtg.WarmNet()
         net.load(WEIGHTS)
-        # the network's activation buffers for this volume are allocated once,
-        # outside the timed region (like the A table and the coarse context)
-        shape = (ctx.N_time, ctx.N_y, ctx.N_x, ctx.N_z)
-        z3 = [torch.zeros(shape, device="cuda") for _ in range(3)]
-        net.forward(z3[0], z3[1], z3[2], shape)
-        del z3
+        # the network's activation buffers and the start images for this
+        # volume are allocated once, outside the timed region (like the A table
+        # and the coarse context): one learned start with a single coarse
+        # iteration
+        ctx.init_learned(net, 1)
     # the coarse context of the multi-resolution start is built once, outside
     # the timed region (like the fine context and its A table)
     ctx.init_multires(1)

@@ -74,6 +74,7 @@ struct xtc_net {
   // activations (BF16) and gradients (FP32) for the current batch shape
   int nb = 0, Y = 0, X = 0, Z = 0;
   Buf in0, a[kLayers], u0, u1, u2, p0, p1, p2, g32, gtmp, gskip[3], gpre;
+  Buf start;  // the learned start's three images (xtg_warm.cu), kept between calls
 };
 
 namespace {
@@ -414,6 +415,17 @@ int xtc_net_load(xtc_net *n, const char *path) {
   }
   return xtc_net_set_params(n, h.data());
 }
+
+}  // extern "C"
+
+// a device buffer of at least `floats` FP32 values owned by the network and
+// kept until it is destroyed (grown when a larger volume asks for more)
+float *xtc_net_start_buffer(xtc_net *n, size_t floats) {
+  if (!n || n->start.ensure(floats * sizeof(float)) != cudaSuccess) return nullptr;
+  return n->start.as<float>();
+}
+
+extern "C" {
 
 int xtc_net_forward(xtc_net *n, const float *fbp, const float *icd, float *out, int32_t nb, int32_t Y, int32_t X,
                     int32_t Z) {

@@ -7,6 +7,7 @@
 #include "../../include/xtg_cnn.h"
 
 void xtg_set_error_text(const char *msg);
+float *xtc_net_start_buffer(xtc_net *n, size_t floats);  // cnn_net.cu
 
 extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coarse_iters, int32_t *used,
                                        double *cost_net, double *cost_base) {
@@ -20,12 +21,11 @@ extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coars
     return XTG_E_ARG;
   }
   const size_t nvox = (size_t)N_time * N_y * N_x * N_z;
-  float *buf = nullptr;
-  cudaError_t e = cudaMalloc(&buf, 3 * nvox * sizeof(float));
-  if (e != cudaSuccess) {
-    char b[200];
-    snprintf(b, sizeof b, "xtg_init_object_learned: %s", cudaGetErrorString(e));
-    xtg_set_error_text(b);
+  // the three images live in a buffer the network keeps, so repeated starts
+  // on one geometry allocate nothing
+  float *buf = xtc_net_start_buffer(net, 3 * nvox);
+  if (!buf) {
+    xtg_set_error_text("xtg_init_object_learned: out of device memory for the start images");
     return XTG_E_CUDA;
   }
   float *fbp = buf, *icd = buf + nvox, *out = buf + 2 * nvox;
@@ -47,7 +47,6 @@ extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coars
     use = cn < ci * (1.0 - 1e-9);
     if (!use && ((rc = xtg_object_from_device(ctx, icd)) || (rc = xtg_init_error_sino(ctx)))) break;
   } while (0);
-  cudaFree(buf);
   if (rc) return rc;
   if (used) *used = use;
   if (cost_net) *cost_net = cn;
