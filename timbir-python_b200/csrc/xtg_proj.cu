@@ -63,6 +63,8 @@ __global__ void __launch_bounds__(FP_WARPS * 32) k_fp_bins(DevGeo G, FpArgs F) {
   extern __shared__ __align__(16) unsigned char fp_sm[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   ACC *acc = reinterpret_cast<ACC *>(fp_sm) + (size_t)warp * 32 * 64;  // [32 bins][64 rows]
+  // the A entries of the warp's 32 candidate columns, [lane][NS]
+  float *vsm = reinterpret_cast<float *>(fp_sm + (size_t)FP_WARPS * 32 * 64 * sizeof(ACC)) + (size_t)warp * 32 * NS;
   const int p = blockIdx.x;
   const int rb = (blockIdx.y * FP_WARPS + warp) * 32;
   const int t0 = blockIdx.z * 64, nt = min(64, G.N_t - t0);
@@ -89,15 +91,26 @@ __global__ void __launch_bounds__(FP_WARPS * 32) k_fp_bins(DevGeo G, FpArgs F) {
     for (int kb = klo; kb <= khi; kb += 32) {
       const int k = kb + lane;
       float v[NS];
+#pragma unroll
+      for (int s = 0; s < NS; s++) v[s] = 0.f;
       int first = 0, n = 0;
       if (k <= khi) n = xt_amatrix_regs<NS>(G, H, cp, sp, j, k, v, &first);
       // entries of this lane's column that land on the warp's bins
       const int slo = max(0, rb - first), shi = min(n, rb + 32 - first);
       const unsigned hit = __ballot_sync(0xffffffffu, slo < shi);
+      if (!hit) continue;
+      // each column's entries go to shared memory, its (first - rb, slo, shi)
+      // into one word, so a hit column costs one shuffle and its entries that
+      // land on the warp's bins are read by a loop over exactly those
+#pragma unroll
+      for (int s = 0; s < NS; s++) vsm[lane * NS + s] = v[s];
+      // for a hit column first - rb lies in (-NS, 32), so the +64 keeps it positive
+      const int pk = (int)(((unsigned)(first - rb + 64) << 16) | ((unsigned)slo << 8) | (unsigned)shi);
+      __syncwarp();
       unsigned mk = hit;
       // the z-line of the next hit column is loaded while the current one is added
       float xa = 0.f, xb = 0.f;
-      if (mk) {
+      {
         const float *xp = xrow + (size_t)(kb + __ffs(mk) - 1) * G.N_z;
         xa = va ? __ldg(xp + za) : 0.f;
         xb = vb ? __ldg(xp + zb2) : 0.f;
@@ -105,29 +118,30 @@ __global__ void __launch_bounds__(FP_WARPS * 32) k_fp_bins(DevGeo G, FpArgs F) {
       while (mk) {
         const int l = __ffs(mk) - 1;
         mk &= mk - 1;
-        const int fl = __shfl_sync(0xffffffffu, first, l);
-        const int sl = __shfl_sync(0xffffffffu, slo, l), sh = __shfl_sync(0xffffffffu, shi, l);
+        const int q = __shfl_sync(0xffffffffu, pk, l);
+        const int sl = (q >> 8) & 0xFF, sh = q & 0xFF;
         const float ca = xa, cb = xb;
         if (mk) {
           const float *xp = xrow + (size_t)(kb + __ffs(mk) - 1) * G.N_z;
           xa = va ? __ldg(xp + za) : 0.f;
           xb = vb ? __ldg(xp + zb2) : 0.f;
         }
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-          const float a = __shfl_sync(0xffffffffu, v[s], l);
-          if (s >= sl && s < sh && a != 0.f) {
-            ACC *q = acc + (fl + s - rb) * 64;
+        ACC *qa = acc + ((q >> 16) - 64 + sl) * 64;
+        const float *vl = vsm + l * NS;
+        for (int s = sl; s < sh; s++, qa += 64) {
+          const float a = vl[s];
+          if (a != 0.f) {
             if (MODE <= 1) {
-              q[ta] = __fadd_rn(q[ta], __fmul_rn(ca, a));
-              q[tb] = __fadd_rn(q[tb], __fmul_rn(cb, a));
+              qa[ta] = __fadd_rn(qa[ta], __fmul_rn(ca, a));
+              qa[tb] = __fadd_rn(qa[tb], __fmul_rn(cb, a));
             } else {
-              q[ta] += (ACC)ca * (ACC)a;
-              q[tb] += (ACC)cb * (ACC)a;
+              qa[ta] += (ACC)ca * (ACC)a;
+              qa[tb] += (ACC)cb * (ACC)a;
             }
           }
         }
       }
+      __syncwarp();  // the staged entries are rewritten by the next round
     }
   }
   __syncwarp();
@@ -165,7 +179,8 @@ __global__ void __launch_bounds__(FP_WARPS * 32) k_fp_bins(DevGeo G, FpArgs F) {
 
 template <int MODE, typename ACC>
 static cudaError_t launch_fp_t(const DevGeo &G, const FpArgs &F, int ns, cudaStream_t st) {
-  const size_t smem = (size_t)FP_WARPS * 32 * 64 * sizeof(ACC);
+  const int nsv = ns <= 3 ? 3 : ns <= 4 ? 4 : 12;
+  const size_t smem = (size_t)FP_WARPS * 32 * 64 * sizeof(ACC) + (size_t)FP_WARPS * 32 * nsv * sizeof(float);
   dim3 grid((unsigned)G.N_p, (unsigned)((G.N_r + FP_WARPS * 32 - 1) / (FP_WARPS * 32)), (unsigned)((G.N_t + 63) / 64));
   typedef void (*K)(DevGeo, FpArgs);
   K k = ns <= 3 ? k_fp_bins<MODE, ACC, 3> : ns <= 4 ? k_fp_bins<MODE, ACC, 4> : k_fp_bins<MODE, ACC, 12>;
