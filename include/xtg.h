@@ -109,6 +109,13 @@ int xtg_get_zslab(const xtg_ctx *ctx, int32_t *slices);
  * XT_Engine.c:89-121): y, w and the offset d (NULL = zero).  Weights are
  * divided by the variance estimate on the device, like the reference. */
 int xtg_upload_sino(xtg_ctx *ctx, const float *y, const float *w, const float *d);
+/* xtg_upload_sino followed by xtg_init_error_sino for the object on the
+ * device (e = y - Ax - d, bit-identical), with the host-to-device copies of
+ * y, w and d on a second stream while Ax is projected.  Host buffers in
+ * pinned memory let the copies overlap.  No XT_Engine counterpart (the
+ * reference reads the sinogram and initialises e as two steps, XT_Engine.c
+ * computeWriteSinogram and XT_ICD_update.c initErrorSinogam). */
+int xtg_upload_sino_start(xtg_ctx *ctx, const float *y, const float *w, const float *d);
 /* Counts ingest, genSinogram_subsampleCounts (XT_genSinogram.c:303-374):
  * bright [N_r*mult_xy][N_t*mult_z] and weight counts [N_p][N_r*mult_xy][N_t*mult_z]
  * are binned to y = log(bright/counts) (+ BH_QUAD_COEF * y^2) and w = counts. */

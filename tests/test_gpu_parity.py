@@ -103,6 +103,44 @@ def test_error_sinogram_and_cost(name):
     assert c.resync_fp64()[0] == pytest.approx(cost, rel=1e-12)
 
 
+@pytest.mark.parametrize("name", ["plain3d", "timbir4d", "offset_zero_mean"])
+def test_upload_sino_start_matches_two_step(name):
+    """xtg_upload_sino_start (copies on a second stream while Ax is projected)
+    leaves e, w and the cost bit-identical to xtg_upload_sino followed by
+    xtg_init_error_sino; twice in a row, from NumPy and from pinned tensors."""
+    import torch
+    c, g, _ = ctx_for(name)
+    d = None
+    if name == "offset_zero_mean":  # a non-zero offset d[N_r][N_t]
+        d = np.random.default_rng(3).normal(0, 0.01, c.sino_shape[1:]).astype(np.float32)
+    c.upload_object(g["x_true"])
+    c.upload_sino(g["y"], g["w"], d)
+    c.init_error_sino()
+    e_ref, w_ref, cost_ref = c.error_sino(), c.weight(), c.cost()[0]
+    for rep in range(2):
+        c.upload_object(g["x_true"] * 0.5)
+        c.init_error_sino()  # a different e in between
+        if rep == 0:
+            c.upload_sino_start(g["y"], g["w"], d)
+        else:
+            t = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory() if a is not None else None
+                 for a in (g["y"], g["w"], d)]
+            c.upload_object(g["x_true"])
+            c.upload_sino_start(*t)
+        if rep == 0:
+            # the object was x_true / 2 when e was formed: compare with that
+            c2, _, _ = ctx_for(name)
+            c2.upload_object(g["x_true"] * 0.5)
+            c2.upload_sino(g["y"], g["w"], d)
+            c2.init_error_sino()
+            assert np.array_equal(c.error_sino(), c2.error_sino())
+            assert np.array_equal(c.weight(), c2.weight())
+        else:
+            assert np.array_equal(c.error_sino(), e_ref)
+            assert np.array_equal(c.weight(), w_ref)
+            assert c.cost()[0] == pytest.approx(cost_ref, rel=1e-12)  # FP64 sums, atomic order
+
+
 def test_zinger_refresh_matches_definition():
     c, g, p = ctx_for("zinger_nhicd")
     c.upload_sino(g["y"], g["w"])

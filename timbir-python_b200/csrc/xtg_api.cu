@@ -94,6 +94,8 @@ struct xtg_ctx {
   int coarse_flags = 0;           // the XTG_MULTIRES_* flags it was built for
   int zslab_req = 0;  // z slices per ICD work piece; 0 = from the L2 size
   cudaStream_t st = nullptr;
+  cudaStream_t st_copy = nullptr;               // host-to-device copies that overlap the projector
+  cudaEvent_t ev_y = nullptr, ev_w = nullptr;  // ... and their completion on it
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
   std::vector<cudaEvent_t> tev;  // start/stop pairs of the ICD launches of one iteration
   int have_sino = 0;
@@ -551,6 +553,9 @@ void xtg_destroy(xtg_ctx *c) {
   for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
   if (c->ek1) cudaEventDestroy(c->ek1);
   if (c->st) cudaStreamDestroy(c->st);
+  if (c->st_copy) cudaStreamDestroy(c->st_copy);
+  if (c->ev_y) cudaEventDestroy(c->ev_y);
+  if (c->ev_w) cudaEventDestroy(c->ev_w);
   xt_views_free(&c->v);
   delete c;
 }
@@ -764,6 +769,45 @@ int xtg_upload_sino(xtg_ctx *c, const float *y, const float *w, const float *d) 
     CK(cudaMemsetAsync(c->d_d, 0, c->nrt * 4, c->st));
   k_scale_weights<<<std::min<unsigned>(blocks_for(c->ns, 256), 4096), 256, 0, c->st>>>(c->ns, c->d_w, c->d_var);
   c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  c->have_sino = 1;
+  return 0;
+}
+
+// e = y - ax - d from ax already in e, in the order the projector's MODE 1
+// applies it (so the result is bit-identical to it)
+__global__ void k_e_from_ax(size_t ns, size_t nrt, const float *__restrict__ y, const float *__restrict__ d,
+                            float *__restrict__ e) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < ns; i += (size_t)gridDim.x * blockDim.x)
+    e[i] = __fsub_rn(__fsub_rn(y[i], e[i]), d[i % nrt]);
+}
+
+int xtg_upload_sino_start(xtg_ctx *c, const float *y, const float *w, const float *d) {
+  if (!c || !y || !w) {
+    set_err("xtg_upload_sino_start: null argument");
+    return XTG_E_ARG;
+  }
+  if (!c->st_copy) CK(cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
+  if (!c->ev_y) CK(cudaEventCreateWithFlags(&c->ev_y, cudaEventDisableTiming));
+  if (!c->ev_w) CK(cudaEventCreateWithFlags(&c->ev_w, cudaEventDisableTiming));
+  // Ax of the resident object on the engine's stream (it reads neither y, w
+  // nor d) while the measurement crosses on the copy stream
+  CK(launch_fp<0>(c, c->d_e, nullptr));
+  CK(cudaMemcpyAsync(c->d_y, y, c->ns * 4, cudaMemcpyHostToDevice, c->st_copy));
+  if (d)
+    CK(cudaMemcpyAsync(c->d_d, d, c->nrt * 4, cudaMemcpyHostToDevice, c->st_copy));
+  else
+    CK(cudaMemsetAsync(c->d_d, 0, c->nrt * 4, c->st_copy));
+  CK(cudaEventRecord(c->ev_y, c->st_copy));
+  CK(cudaMemcpyAsync(c->d_w, w, c->ns * 4, cudaMemcpyHostToDevice, c->st_copy));
+  CK(cudaEventRecord(c->ev_w, c->st_copy));
+  CK(cudaStreamWaitEvent(c->st, c->ev_y, 0));
+  k_e_from_ax<<<std::min<unsigned>(blocks_for(c->ns, 256), (unsigned)c->sm_count * 8), 256, 0, c->st>>>(
+      c->ns, c->nrt, c->d_y, c->d_d, c->d_e);
+  CK(cudaStreamWaitEvent(c->st, c->ev_w, 0));
+  k_scale_weights<<<std::min<unsigned>(blocks_for(c->ns, 256), 4096), 256, 0, c->st>>>(c->ns, c->d_w, c->d_var);
+  c->launches += 2;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
   c->have_sino = 1;

@@ -28,7 +28,7 @@ XTG_MULTIRES_Z, XTG_MULTIRES_BIN = 1, 2
 XTG_SYMBOLS = [
     "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_init_object_fbp", "xtg_object_to_device",
     "xtg_object_from_device", "xtg_upsample", "xtg_init_object_multires", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
-    "xtg_get_hr", "xtg_set_options", "xtg_upload_sino", "xtg_upload_counts", "xtg_upload_object",
+    "xtg_get_hr", "xtg_set_options", "xtg_upload_sino", "xtg_upload_sino_start", "xtg_upload_counts", "xtg_upload_object",
     "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
     "xtg_get_offset", "xtg_set_offset", "xtg_get_magmap", "xtg_set_magmap", "xtg_get_variance",
     "xtg_set_variance", "xtg_amatrix", "xtg_forward_project", "xtg_init_error_sino",
@@ -336,6 +336,17 @@ class Context:
         y, w = _f32(y), _f32(w)
         d = None if d is None else _f32(d)
         _check(self.lib.xtg_upload_sino(self.h, _p(y), _p(w), _p(d)), "xtg_upload_sino")
+
+    def upload_sino_start(self, y, w, d=None):
+        """upload_sino + init_error_sino for the resident object, the copies
+        overlapping the projection (pinned torch CPU tensors overlap best)."""
+        if hasattr(y, "data_ptr"):
+            ptrs = [C.c_void_p(t.data_ptr()) if t is not None else None for t in (y, w, d)]
+        else:
+            y, w = _f32(y), _f32(w)
+            d = None if d is None else _f32(d)
+            ptrs = [_p(y), _p(w), _p(d)]
+        _check(self.lib.xtg_upload_sino_start(self.h, *ptrs), "xtg_upload_sino_start")
 
     def upload_counts(self, bright, counts, bh=0.0, d=None):
         b, c = _f32(bright), _f32(counts)
