@@ -461,8 +461,9 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
     }
-    if not args.no_converge:
-        # the committed warm-start weights were trained for the plain-3D geometry
+    if not args.no_converge and world == 1:
+        # a single-GPU metric: with N replicas every rank would repeat it.
+        # The committed warm-start weights were trained for the plain-3D geometry
         line["time_to_cost"] = converge(ctx, args.amode, learned=args.workload == "plain3d" and not args.nxy)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
