@@ -31,7 +31,8 @@ int xtc_conv3d(const void *in, const void *w, const float *bias, void *out, int3
 /* xtc_conv3d with the kernel chosen: XTC_CONV_AUTO (what xtc_conv3d does), XTC_CONV_GATHER (operands
  * gathered per K stage by the CTA's threads) or XTC_CONV_TILE (input tile staged once by TMA, every tap
  * a shifted view of it; X a multiple of 128, Z even, cout <= 64, else XTG_E_ARG).  The tile kernel is
- * used by AUTO wherever it applies. */
+ * used by AUTO wherever it applies.  Its packed weights go to one buffer the library keeps: calls from
+ * several host threads must be serialised. */
 enum { XTC_CONV_AUTO = 0, XTC_CONV_GATHER = 1, XTC_CONV_TILE = 2 };
 int xtc_conv3d_path(const void *in, const void *w, const float *bias, void *out, int32_t nb, int32_t Y, int32_t X,
                     int32_t Z, int32_t cin, int32_t cout, int32_t kpad, int32_t epi, int32_t sign, int32_t path);
