@@ -243,7 +243,9 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     region) and is timed on the wall clock, cost test included: after every
     iteration the MAP cost of the running error sinogram (FP64 sums), every
     `resync_every` iterations and at the stop the FP64 resync; it stops at the
-    first FP64-resynced cost <= (1 + tol) C*."""
+    first FP64-resynced cost <= (1 + tol) C*.  After each pass (outside its
+    timed region) its object is compared with the C* object: `rmse_rel` =
+    RMS difference / max |x*|."""
     import torch
     zero = np.zeros(ctx.obj_shape, np.float32)
     torch.cuda.synchronize()
@@ -256,6 +258,8 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
         if it >= 20 and (hist[-11] - hist[-1]) < stall * abs(hist[-1]):
             break
     c_star = ctx.resync_fp64()[0]
+    x_star = ctx.object()
+    x_scale = float(np.abs(x_star).max()) or 1.0
     out = {"c_star": c_star, "c_star_iterations": len(hist), "tol": tol,
            "c_star_source": "this engine from the FBP start run to a stall (FP64 resync cost); at test sizes "
                             "the parallel schedule reaches the FP64 CPU oracle's converged cost"}
@@ -305,7 +309,8 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
                     break
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
-        out[kind] = {"s": secs if c <= target else None, "iterations": it, "cost": c,
+        rmse = float(np.sqrt(np.mean((ctx.object() - x_star) ** 2))) / x_scale
+        out[kind] = {"s": secs if c <= target else None, "iterations": it, "cost": c, "rmse_rel": rmse,
                      "a_mode": {v: k for k, v in AMODES.items()}[am], **extra}
     if net is not None:
         out["network"] = network_roofline(ctx, net, coarse_iters)
