@@ -1178,7 +1178,10 @@ int xtg_init_error_sino(xtg_ctx *c) {
 
 static int finish_cost(xtg_ctx *c, double data_sum, double *cost, double *fwd, double *prior);
 
-int xtg_init_object_fbp(xtg_ctx *c) {
+// the FBP image into the object, leaving e stale (filtered sinogram in it):
+// for callers inside the library that replace the object again before they
+// iterate (not exported)
+__attribute__((visibility("hidden"))) int xtg_fbp_image_only(xtg_ctx *c) {
   if (!c) return XTG_E_ARG;
   if (!c->have_sino) {
     set_err("xtg_init_object_fbp: no sinogram uploaded");
@@ -1188,7 +1191,12 @@ int xtg_init_object_fbp(xtg_ctx *c) {
   CK(launch_fbp(c->G, c->d_y, c->d_d, c->d_e, c->d_cos, c->d_sin, c->d_view_idx, c->d_view_start, c->d_view_num,
                 c->d_rank, c->d_x, c->st));
   c->launches += 2;
-  return xtg_init_error_sino(c);
+  return 0;
+}
+
+int xtg_init_object_fbp(xtg_ctx *c) {
+  const int rc = xtg_fbp_image_only(c);
+  return rc ? rc : xtg_init_error_sino(c);
 }
 
 int xtg_resync_fp64(xtg_ctx *c, double *cost, double *fwd, double *prior) {

@@ -8,6 +8,7 @@
 
 void xtg_set_error_text(const char *msg);
 float *xtc_net_start_buffer(xtc_net *n, size_t floats);  // cnn_net.cu
+extern "C" int xtg_fbp_image_only(xtg_ctx *c);             // xtg_api.cu
 
 extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coarse_iters, int32_t *used,
                                        double *cost_net, double *cost_base) {
@@ -32,7 +33,8 @@ extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coars
   double ci = 0, cn = 0;
   int use = 0;
   do {
-    if ((rc = xtg_init_object_fbp(ctx)) || (rc = xtg_object_to_device(ctx, fbp))) break;
+    // the FBP image only: the multi-resolution start below recomputes e
+    if ((rc = xtg_fbp_image_only(ctx)) || (rc = xtg_object_to_device(ctx, fbp))) break;
     // the multi-resolution start (it ends with e = y - Ax - d recomputed, so
     // both candidates are costed from a fresh e)
     if ((rc = xtg_init_object_multires(ctx, coarse_iters, N_z % 2 == 0 && N_z >= 16)) ||
