@@ -5,7 +5,7 @@ holds the reference's FP64 cost per iteration for 150 iterations, the last
 being its converged cost C*, its FP32 costs for the 20 equits, and its
 converged object).
 
-Criteria (the reconstruction is judged by the reference's MAP cost):
+Criteria (the reconstruction is measured by the reference's MAP cost):
   * after the configuration's 20 iterations the GPU's FP64 cost is within
     1e-4 of C* -- what the reference reaches at iteration 19;
   * the parallel schedule needs at most twice the reference's iterations to

@@ -10,7 +10,7 @@ Tolerances, stated per test:
     vs the reference: object within 1e-4 relative of its range (the only
     difference is the summation order of theta1/theta2);
   * parallel ICD: MAP cost within 1e-4 relative of the FP64 oracle's
-    converged cost -- the north-star convergence criterion.
+    converged cost, and RMSE against its converged object.
 """
 import os
 
