@@ -54,6 +54,8 @@ void xtg_set_error_text(const char *msg) { snprintf(g_err, sizeof g_err, "%s", m
 // parallel ICD: at most 1 in XTG_CONC_DIV of the columns updated at once
 #define XTG_CONC_DIV 32
 
+struct RsState;  // radix-select state per segment (defined with its kernels)
+
 struct xtg_ctx {
   xt_params prm;
   xt_geom g;
@@ -71,6 +73,8 @@ struct xtg_ctx {
   int *d_view_idx = nullptr, *d_view_start = nullptr, *d_view_num = nullptr, *d_fov = nullptr;
   int *d_mcols = nullptr, *d_rank = nullptr, *d_counter = nullptr, *d_nhcnt = nullptr, *d_err = nullptr;
   int *d_kth = nullptr;
+  unsigned *d_rs_hist = nullptr;  // [segments][256] radix-select histograms
+  RsState *d_rs_st = nullptr;     // [segments]
   int4 *d_items = nullptr, *d_nh = nullptr;
   size_t items_cap = 0, nh_cap = 0;
   double *d_red = nullptr;       // [8][NSLOT] reduction slots
@@ -296,6 +300,67 @@ __global__ void __launch_bounds__(1024) k_radix_select(const float *vals, int se
     __syncthreads();
   }
   if (threadIdx.x == 0) out[blockIdx.x] = xt_key2f(s_prefix);
+}
+
+// The same order statistic spread over many CTAs per segment: per 8-bit pass,
+// k_rs_hist counts the keys that match the prefix found so far into a global
+// 256-bin histogram of the segment (a warp whose lanes share one bin adds 32
+// with a single atomic), and k_rs_pick finds the bin that holds the k-th key,
+// narrows the prefix and clears the histogram for the next pass.
+struct RsState {
+  unsigned prefix, mask, k, pad;
+};
+
+__global__ void k_rs_init(const int *kth, RsState *st, unsigned *hist) {
+  if (threadIdx.x == 0) st[blockIdx.x] = RsState{0u, 0u, (unsigned)kth[blockIdx.x], 0u};
+  for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[(size_t)blockIdx.x * 256 + b] = 0u;
+}
+
+__global__ void __launch_bounds__(256) k_rs_hist(const float *vals, int seglen, int shift, const RsState *st,
+                                                 unsigned *hist) {
+  __shared__ unsigned h[256];
+  const int seg = blockIdx.y, lane = threadIdx.x & 31;
+  h[threadIdx.x] = 0u;
+  __syncthreads();
+  const unsigned pre = st[seg].prefix, msk = st[seg].mask;
+  const float *v = vals + (size_t)seg * seglen;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x - lane; i0 < seglen; i0 += stride) {
+    const int i = i0 + lane;
+    unsigned bin = 256u;  // no key here, or not under the prefix
+    if (i < seglen) {
+      const unsigned key = xt_f2key(v[i]);
+      if ((key & msk) == pre) bin = (key >> shift) & 255u;
+    }
+    const unsigned b0 = __shfl_sync(0xffffffffu, bin, 0);
+    if (__all_sync(0xffffffffu, bin == b0)) {
+      if (lane == 0 && b0 < 256u) atomicAdd(&h[b0], 32u);
+    } else if (bin < 256u) {
+      atomicAdd(&h[bin], 1u);
+    }
+  }
+  __syncthreads();
+  if (h[threadIdx.x]) atomicAdd(&hist[(size_t)seg * 256 + threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_rs_pick(int shift, RsState *st, unsigned *hist, float *out) {
+  const int seg = blockIdx.x;
+  unsigned *hs = hist + (size_t)seg * 256;
+  if (threadIdx.x == 0) {
+    const unsigned k = st[seg].k;
+    unsigned cum = 0;
+    int b = 0;
+    for (; b < 255; b++) {
+      if (cum + hs[b] >= k) break;
+      cum += hs[b];
+    }
+    st[seg].k = k - cum;
+    st[seg].prefix |= (unsigned)b << shift;
+    st[seg].mask |= 255u << shift;
+    if (shift == 0) out[seg] = xt_key2f(st[seg].prefix);
+  }
+  __syncthreads();
+  hs[threadIdx.x] = 0u;
 }
 
 // columns above the threshold -> NHICD work items.  List 0 holds the
@@ -544,7 +609,7 @@ void xtg_destroy(xtg_ctx *c) {
                   c->d_filt, c->d_tmp, c->d_num, c->d_den, c->d_thr, c->d_var, c->d_view_idx, c->d_view_start,
                   c->d_view_num, c->d_fov, c->d_mcols, c->d_rank, c->d_counter, c->d_nhcnt, c->d_err, c->d_kth,
                   c->d_items, c->d_nh, c->d_red, c->d_absx, c->d_cnt, c->d_tstart, c->d_toff, c->d_tval32,
-                  c->d_tscale, c->d_tval16};
+                  c->d_tscale, c->d_tval16, c->d_rs_hist, c->d_rs_st};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -639,6 +704,8 @@ int xtg_create(const xt_params *prm, const double *times, const double *angles, 
   rc |= dalloc(c, &c->d_den, c->nrt);
   rc |= dalloc(c, &c->d_thr, (size_t)g.N_time * g.nzb);
   rc |= dalloc(c, &c->d_kth, (size_t)g.N_time * g.nzb);
+  rc |= dalloc(c, &c->d_rs_hist, (size_t)g.N_time * g.nzb * 256);
+  rc |= dalloc(c, &c->d_rs_st, (size_t)g.N_time * g.nzb);
   rc |= dalloc(c, &c->d_var, 1);
   rc |= dalloc(c, &c->d_view_idx, (size_t)g.N_p);
   rc |= dalloc(c, &c->d_view_start, (size_t)g.N_time);
@@ -1512,6 +1579,20 @@ static void magsum_launch(xtg_ctx *c) {
   c->launches++;
 }
 
+// k-th smallest of each of nseg segments of c->d_filt (k from c->d_kth) into
+// c->d_thr: four 8-bit passes, each a histogram over many CTAs and a pick
+static void radix_select_multi(xtg_ctx *c, int nseg) {
+  const int seglen = (int)c->nxy;
+  const int parts = std::max(1, std::min(64, (seglen + 8191) / 8192));
+  k_rs_init<<<nseg, 256, 0, c->st>>>(c->d_kth, c->d_rs_st, c->d_rs_hist);
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    k_rs_hist<<<dim3((unsigned)parts, (unsigned)nseg), 256, 0, c->st>>>(c->d_filt, seglen, shift, c->d_rs_st,
+                                                                       c->d_rs_hist);
+    k_rs_pick<<<nseg, 256, 0, c->st>>>(shift, c->d_rs_st, c->d_rs_hist, c->d_thr);
+  }
+  c->launches += 9;
+}
+
 // NHICD selection on the device: filter, per-(frame, block) order statistic,
 // compaction into the two half-pass lists.
 static int nhicd_select_device(xtg_ctx *c) {
@@ -1522,13 +1603,13 @@ static int nhicd_select_device(xtg_ctx *c) {
   CK(cudaMemcpyAsync(c->d_kth, kth.data(), nseg * 4, cudaMemcpyHostToDevice, c->st));
   const unsigned grid = std::min<unsigned>(blocks_for(c->nmag, 256), (unsigned)c->sm_count * 8);
   k_vsc_filter<<<grid, 256, 0, c->st>>>(nseg, g.N_y, g.N_x, c->d_mag, c->d_filt);
-  k_radix_select<<<nseg, 1024, 0, c->st>>>(c->d_filt, (int)c->nxy, c->d_kth, c->d_thr);
+  radix_select_multi(c, nseg);
   CK(cudaMemsetAsync(c->d_nhcnt, 0, 8, c->st));
   const int cap0 = (int)(c->nh_cap / 2), cap1 = (int)(c->nh_cap - c->nh_cap / 2);
   k_nhicd_compact<<<grid, 256, 0, c->st>>>(g.N_time, g.nzb, g.N_y, g.N_x, c->d_filt, c->d_thr, c->d_rank,
                                            c->d_mag, c->d_nh, c->d_nh + cap0, c->d_nhcnt, cap0, cap1);
   k_clamp_count<<<1, 32, 0, c->st>>>(c->d_nhcnt, cap0, cap1);
-  c->launches += 4;
+  c->launches += 3;
   CK(cudaGetLastError());
   return 0;
 }
@@ -1911,8 +1992,8 @@ int xtg_nhicd_select(xtg_ctx *c, const int32_t *usn, int32_t *nnum, int32_t *xse
   CK(cudaMemcpyAsync(c->d_kth, kth.data(), nseg * 4, cudaMemcpyHostToDevice, c->st));
   const unsigned grid = std::min<unsigned>(blocks_for(c->nmag, 256), (unsigned)c->sm_count * 8);
   k_vsc_filter<<<grid, 256, 0, c->st>>>(nseg, g.N_y, g.N_x, c->d_mag, c->d_filt);
-  k_radix_select<<<nseg, 1024, 0, c->st>>>(c->d_filt, (int)c->nxy, c->d_kth, c->d_thr);
-  c->launches += 2;
+  radix_select_multi(c, nseg);
+  c->launches += 1;
   CK(cudaGetLastError());
   std::vector<float> th(nseg), f(c->nmag);
   CK(cudaMemcpyAsync(th.data(), c->d_thr, nseg * 4, cudaMemcpyDeviceToHost, c->st));
