@@ -10,7 +10,8 @@
 //   k_prior_cost64    qGGMRF prior over forward neighbour pairs, FP64
 //   k_running_cost64  data term from the running e, FP64
 //   k_zinger_refresh  ProjSelect = |e sqrt(w)| < T
-//   k_vsc_filter / k_radix_select / k_nhicd_compact   NHICD selection
+//   k_vsc_filter / k_rs_hist + k_rs_pick / k_nhicd_compact   NHICD selection
+//   k_radix_select    the same order statistic in one CTA (allocation-free path)
 //   k_offset_* / k_var_*   offset d and variance re-estimation
 //   k_build_items / k_magsum / k_build_a16 / k_counts / object transposes
 #include <algorithm>
