@@ -2,7 +2,8 @@
 routines compiled from its sources (oracle/_ref), live, on seeded random
 geometries beyond the committed fixtures: detector sizes, view counts,
 delta_xy / delta_z of 1 and 2, rotation centres off the middle, zinger
-correction and NHICD on and off, offset re-estimation.  Skipped where the
+correction and NHICD on and off, offset re-estimation; and 4D cases of 2-3
+frames of interlaced views with moving objects.  Skipped where the
 reference build is absent (the committed fixtures pin the oracle there).
 
 Single-threaded, so everything is compared bit for bit: the geometry
@@ -40,12 +41,22 @@ def random_case(seed):
     return pk, dk
 
 
-@pytest.mark.parametrize("seed", range(8))
-def test_oracle_matches_reference_live(seed, tmp_path, monkeypatch):
-    pk, dk = random_case(seed)
+def random_case_4d(seed):
+    """Frames of interlaced views (the launcher's bit-reversed sub-frames) and
+    a phantom with moving ellipsoids."""
+    rng = np.random.default_rng(1000 + seed)
+    n_time = int(rng.choice([2, 3]))
+    K, N_theta = [(4, 16), (2, 8)][int(rng.integers(0, 2))]
+    N = int(rng.choice([12, 16]))
+    pk = dict(N=N, NT=2, NP=n_time * N_theta, n_time=n_time, nhicd=bool(rng.integers(0, 2)))
+    dk = dict(seed=200 + seed, moving=2)
+    return pk, dk, (K, N_theta)
+
+
+def compare(pk, dk, interlaced, seed, tmp_path, monkeypatch):
     p = common.params(**pk)
     monkeypatch.chdir(tmp_path)
-    t, a = common.views(p)
+    t, a = common.views(p, interlaced)
     xtg.write_view_file("view_info.txt", t, a)
     x, _, y, w = common.data(p, t, a, **dk)
     r = Reference(p)
@@ -83,3 +94,15 @@ def test_oracle_matches_reference_live(seed, tmp_path, monkeypatch):
     finally:
         o.close()
         r.close()
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_oracle_matches_reference_live(seed, tmp_path, monkeypatch):
+    pk, dk = random_case(seed)
+    compare(pk, dk, None, seed, tmp_path, monkeypatch)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_oracle_matches_reference_live_4d(seed, tmp_path, monkeypatch):
+    pk, dk, views = random_case_4d(seed)
+    compare(pk, dk, views, seed, tmp_path, monkeypatch)
