@@ -18,7 +18,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
-#include "../timbir-python_b200/csrc/xt_geom.h"
+#include "xt_geom.h"
 
 #ifdef __cplusplus
 extern "C" {

@@ -26,7 +26,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
-#include "../timbir-python_b200/csrc/xt_geom.h"
+#include "xt_geom.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -144,7 +144,12 @@ int xtg_amatrix(xtg_ctx *ctx, int32_t n, const int32_t *rows, const int32_t *col
  * XT_ICD_update.c:551-569, XT_ForwardProject.c:8-25).  ax may be NULL
  * (result stays on the device). */
 int xtg_forward_project(xtg_ctx *ctx, float *ax);
-/* e = y - A x - d in FP32 (initErrorSinogam, XT_ICD_update.c:538-597). */
+/* e = y - A x - d in FP32 (initErrorSinogam, XT_ICD_update.c:538-597), with
+ * the reference's projector, which leaves out the delta_t factor the voxel
+ * update applies to A (XT_ForwardProject.c:17 against XT_VoxUpdate.c:27,67):
+ * with delta_t != 1 only a zero object gives the e the update assumes, in
+ * the reference as here.  The starts this library computes itself (FBP,
+ * multi-resolution, learned) set e = y - A delta_t x - d instead. */
 int xtg_init_error_sino(xtg_ctx *ctx);
 /* Warm start: object := filtered backprojection of y - d (ramp filter and
  * linearly interpolated backprojection over each frame's views; 0 outside
@@ -181,12 +186,15 @@ int xtg_upsample(xtg_ctx *ctx, const float *in, float *out, int32_t nt, int32_t 
  * with --initICD 2/3). */
 enum { XTG_MULTIRES_Z = 1, XTG_MULTIRES_BIN = 2 };
 int xtg_init_object_multires(xtg_ctx *ctx, int32_t coarse_iters, int32_t flags);
-/* e = y - A x - d with FP64 accumulation, rounded to FP32: the periodic
- * resync that removes the drift of incremental FP32 updates.  The same pass
- * yields the MAP cost of the current object in FP64 (outputs may be NULL). */
+/* e = y - A delta_t x - d with FP64 accumulation, rounded to FP32: the
+ * periodic resync that removes the drift of incremental FP32 updates.  A
+ * delta_t is the matrix the voxel update subtracts (XT_VoxUpdate.c:27,67), so
+ * this is the error sinogram the reference carries from its zero start.  The
+ * same pass yields the MAP cost of the current object in FP64 (outputs may be
+ * NULL). */
 int xtg_resync_fp64(xtg_ctx *ctx, double *cost, double *forward, double *prior);
 /* MAP cost of the current object (computeCost, XT_ICD_update.c:181-314),
- * evaluated in FP64 from e64 = y - A x - d (not from the running e). */
+ * evaluated in FP64 from e64 = y - A delta_t x - d (not from the running e). */
 int xtg_map_cost_fp64(xtg_ctx *ctx, double *cost, double *forward, double *prior);
 /* MAP cost from the running error sinogram in FP64 arithmetic. */
 int xtg_map_cost_running(xtg_ctx *ctx, double *cost, double *forward, double *prior);

@@ -246,6 +246,21 @@ class Oracle(_Base):
         self._call("forward_project", C.c_void_p(self.h), o)
         return o
 
+    def map_cost_fp64(self):
+        """MAP cost of the object, every sum in FP64 (this build's A and
+        constants): (cost, forward, prior)."""
+        fn = self.lib.xo_map_cost_fp64
+        fn.restype = C.c_double
+        fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        f, p = C.c_double(), C.c_double()
+        c = fn(C.c_void_p(self.h), C.byref(f), C.byref(p))
+        return float(c), float(f.value), float(p.value)
+
+    def init_error_sino_model(self):
+        """e = y - delta_t A x - d (the voxel update's matrix)."""
+        self.lib.xo_init_error_sino_model.argtypes = None
+        self._call("init_error_sino_model", C.c_void_p(self.h))
+
     def iterate(self, it):
         pct = self.creal()
         f = self.lib.xo_iterate(C.c_void_p(self.h), it, C.byref(pct))
@@ -279,7 +294,13 @@ class Reference(_Base):
     prefix = "xr_"
 
     def __init__(self, params, double=False):
-        lib = _lib(os.path.join(REF_DIR, "libxtref64.so" if double else "libxtref32.so"))
+        if getattr(params, "positivity", 1):
+            name = "libxtref64.so" if double else "libxtref32.so"
+        elif not double:
+            name = "libxtref32_nopos.so"  # the reference built without POSITIVITY_CONSTRAINT
+        else:
+            raise ValueError("no FP64 reference build without positivity")
+        lib = _lib(os.path.join(REF_DIR, name))
         lib.xr_create.restype = C.c_void_p
         argv = ["XT_Engine"] + params.cli()
         self._argv = (C.c_char_p * len(argv))(*[s.encode() for s in argv])

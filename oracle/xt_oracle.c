@@ -398,15 +398,19 @@ void xo_set_error_sino(xo_ctx *c, const xo_real *e) {
 /* ------------------------------------------------- forward projection ---- */
 /* initErrorSinogam first half + forward_project_voxel_AMat1D,
  * XT_ICD_update.c:551-569, XT_ForwardProject.c:8-25 */
+/* Each view's sinogram entries receive their terms in the reference's
+ * (row, column) order, so running the views on separate threads changes no
+ * bit of the result. */
 void xo_forward_project(const xo_ctx *c, xo_real *ax) {
-  xo_real vals[16];
-  int32_t idx[16];
   memset(ax, 0, sizeof(xo_real) * (size_t)c->N_p * c->N_r * c->N_t);
-  for (int i = 0; i < c->N_time; i++)
-    for (int j = 0; j < c->N_y; j++)
-      for (int k = 0; k < c->N_x; k++)
-        for (int pp = 0; pp < c->proj_num[i]; pp++) {
-          int32_t p = c->proj_idx[c->proj_start[i] + pp];
+  for (int i = 0; i < c->N_time; i++) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int pp = 0; pp < c->proj_num[i]; pp++) {
+      xo_real vals[16];
+      int32_t idx[16];
+      const int32_t p = c->proj_idx[c->proj_start[i] + pp];
+      for (int j = 0; j < c->N_y; j++)
+        for (int k = 0; k < c->N_x; k++) {
           int32_t cnt = xo_amatrix(c, j, k, p, vals, idx);
           for (int s = 0; s < c->N_z; s++) {
             xo_real pix = OBJ(c, i, s + 1, j, k);
@@ -414,6 +418,8 @@ void xo_forward_project(const xo_ctx *c, xo_real *ax) {
               for (int n = 0; n < c->zovl; n++) ax[SIDX(c, p, idx[m], s * c->zovl + n)] += pix * vals[m];
           }
         }
+    }
+  }
 }
 
 /* initErrorSinogam, XT_ICD_update.c:538-597 */
@@ -428,6 +434,21 @@ void xo_init_error_sino(xo_ctx *c) {
         c->sel[q] = xo_select(c, c->e[q], c->w[q]);
       }
   (void)ns;
+}
+
+/* e = y - delta_t A x - d: the error sinogram of the matrix the voxel update
+ * subtracts (A * delta_t, XT_VoxUpdate.c:27, 67), which the reference carries
+ * from its zero start; initErrorSinogam's projector leaves delta_t out
+ * (XT_ForwardProject.c:17).  Equal to xo_init_error_sino when delta_t = 1. */
+void xo_init_error_sino_model(xo_ctx *c) {
+  xo_forward_project(c, c->e);
+  for (int p = 0; p < c->N_p; p++)
+    for (int r = 0; r < c->N_r; r++)
+      for (int t = 0; t < c->N_t; t++) {
+        size_t q = SIDX(c, p, r, t);
+        c->e[q] = c->y[q] - c->delta_t * c->e[q] - c->d[(size_t)r * c->N_t + t];
+        c->sel[q] = xo_select(c, c->e[q], c->w[q]);
+      }
 }
 
 /* ------------------------------------------------------------ prior ------ */
@@ -546,6 +567,77 @@ xo_real xo_cost(xo_ctx *c, xo_real *fwd_out, xo_real *prior_out) {
   if (fwd_out) *fwd_out = forward;
   if (prior_out) *prior_out = prior;
   return forward + prior;
+}
+
+/* The MAP cost of the current object with every sum in FP64: e64 =
+ * y - delta_t A x - d from products of this build's A entries (FP32 in the
+ * float build, as the reference's default build computes them), the data
+ * term of computeCost (XT_ICD_update.c:181-200) on e64, and the prior over
+ * the same forward neighbour pairs (XT_ICD_update.c:201-294) with this
+ * build's constants promoted to FP64.  In the float build that is the
+ * arithmetic of the GPU's FP64 MAP cost, term for term; the double build is
+ * the reference's -DREAL_IS_DOUBLE evaluation (A itself in FP64). */
+double xo_map_cost_fp64(const xo_ctx *c, double *fwd_out, double *prior_out) {
+  const size_t ns = (size_t)c->N_p * c->N_r * c->N_t;
+  double *ax = (double *)calloc(ns, sizeof(double));
+  if (!ax) return NAN;
+  for (int i = 0; i < c->N_time; i++) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int pp = 0; pp < c->proj_num[i]; pp++) {
+      xo_real vals[16];
+      int32_t idx[16];
+      const int32_t p = c->proj_idx[c->proj_start[i] + pp];
+      for (int j = 0; j < c->N_y; j++)
+        for (int k = 0; k < c->N_x; k++) {
+          int32_t cnt = xo_amatrix(c, j, k, p, vals, idx);
+          for (int s = 0; s < c->N_z; s++) {
+            const double pix = (double)OBJ(c, i, s + 1, j, k);
+            for (int m = 0; m < cnt; m++)
+              for (int n = 0; n < c->zovl; n++) ax[SIDX(c, p, idx[m], s * c->zovl + n)] += pix * (double)vals[m];
+          }
+        }
+    }
+  }
+  const double T = (double)c->T, dl = (double)c->delta, dt = (double)c->delta_t;
+  double data = 0;
+#pragma omp parallel for reduction(+ : data)
+  for (int p = 0; p < c->N_p; p++)
+    for (int r = 0; r < c->N_r; r++)
+      for (int t = 0; t < c->N_t; t++) {
+        const size_t q = SIDX(c, p, r, t);
+        const double e = (double)c->y[q] - dt * ax[q] - (double)c->d[(size_t)r * c->N_t + t];
+        const double sw = e * sqrt((double)c->w[q]);
+        data += fabs(sw) < T ? sw * sw : 2.0 * dl * T * fabs(sw) + T * T * (1.0 - 2.0 * dl);
+      }
+  free(ax);
+  const double sq = (double)c->Sigma_S_Q, sqp = (double)c->Sigma_S_Q_P, cs = (double)c->C_S;
+  const double tq = (double)c->Sigma_T_Q, tqp = (double)c->Sigma_T_Q_P, ct = (double)c->C_T, mp = (double)c->MRF_P;
+  double prior = 0;
+#pragma omp parallel for reduction(+ : prior)
+  for (int p = 1; p < c->N_z + 1; p++)
+    for (int i = 0; i < c->N_time; i++)
+      for (int j = 0; j < c->N_y; j++)
+        for (int k = 0; k < c->N_x; k++) {
+          const double v = (double)OBJ(c, i, p, j, k);
+          for (int dz = 0; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+              for (int dx = -1; dx <= 1; dx++) {
+                /* the 13 forward pairs: +x in the row, the next row, the next slice */
+                if (dz == 0 && (dy < 0 || (dy == 0 && dx <= 0))) continue;
+                const int jj = j + dy, kk = k + dx, zz = p + dz;
+                if (jj < 0 || jj >= c->N_y || kk < 0 || kk >= c->N_x || zz > c->N_z) continue;
+                const double a = fabs(v - (double)OBJ(c, i, zz, jj, kk));
+                prior += (double)c->SF[1 + dz][1 + dy][1 + dx] * ((a * a / sq) / (cs + pow(a, 2.0 - mp) / sqp));
+              }
+          if (i + 1 < c->N_time) {
+            const double a = fabs(v - (double)OBJ(c, i + 1, p, j, k));
+            prior += (double)c->TF * ((a * a / tq) / (ct + pow(a, 2.0 - mp) / tqp));
+          }
+        }
+  const double fwd = data / 2.0 + (double)c->N_p * c->N_r * c->N_t * log((double)c->var_est) / 2.0;
+  if (fwd_out) *fwd_out = fwd;
+  if (prior_out) *prior_out = prior;
+  return fwd + prior;
 }
 
 /* ------------------------------------------------------ voxel update ----- */

@@ -80,6 +80,10 @@ xo_real xo_get_var(const xo_ctx *c);
 
 void xo_forward_project(const xo_ctx *c, xo_real *ax /*[N_p][N_r][N_t]*/);
 void xo_init_error_sino(xo_ctx *c);
+/* e = y - delta_t A x - d (the voxel update's matrix; see xt_oracle.c) */
+void xo_init_error_sino_model(xo_ctx *c);
+/* MAP cost of the object with FP64 sums (see xt_oracle.c) */
+double xo_map_cost_fp64(const xo_ctx *c, double *fwd, double *prior);
 xo_real xo_cost(xo_ctx *c, xo_real *forward, xo_real *prior);
 
 xo_real xo_functional_substitution(const xo_ctx *c, xo_real V, xo_real th1, xo_real th2,

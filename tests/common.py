@@ -10,10 +10,13 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def params(N=32, NT=4, NP=36, n_time=1, dxy=1.0, dz=1.0, zinger=False, nhicd=False, threads=1, rot=None,
-           positivity=1, sigma=200000.0, c=0.01, alpha=1.0, offset=0, var=0, zero_mean=0, rtime_delta=None):
+           positivity=1, sigma=200000.0, c=0.01, alpha=1.0, offset=0, var=0, zero_mean=0, rtime_delta=None, pitch=1.0):
+    """pitch: detector pitch in length units (length_r = pitch N_r, length_t =
+    pitch N_t); the launcher passes physical lengths, so its delta_r and
+    delta_t differ from 1."""
     return xtg.Params(
-        p=1.2, sigma_s=sigma, sigma_t=sigma, c_s=c, c_t=c, delta_xy=dxy, delta_z=dz, length_r=float(N),
-        length_t=float(NT), rotation_center=float(N) / 2 if rot is None else rot, alpha=alpha, Rtime0=0.0,
+        p=1.2, sigma_s=sigma, sigma_t=sigma, c_s=c, c_t=c, delta_xy=dxy, delta_z=dz, length_r=pitch * float(N),
+        length_t=pitch * float(NT), rotation_center=float(N) / 2 if rot is None else rot, alpha=alpha, Rtime0=0.0,
         Rtime_delta=float(NP // n_time) if rtime_delta is None else rtime_delta, radius_obj=float(N),
         zingerT=4.0 if zinger else 100000.0, zingerDel=0.5 if zinger else 0.0, iter=3,
         Rtime_num=n_time, num_projections=NP, N_r=N, N_t=NT, num_threads=threads, positivity=positivity,

@@ -5,11 +5,12 @@ Each case writes the launcher's input files (view_info.txt, projection /
 weight or bright / counts, and for the multi-resolution stage the coarser
 object, magnitude-update map, offset and variance), runs the reference
 XT_Engine (gromitsun/timbir-python Source_Code_4D_Fast, built by
-`make -C oracle` as oracle/_ref/XT_Engine_ref32) with the launcher's options
+`make -C oracle` as oracle/_ref/XT_Engine_ref32, or XT_Engine_ref32_nopos for a
+case with positivity off) with the launcher's options
 in a scratch directory, and stores every input and output file byte for byte
 together with the argument list:
 
-    python tests/golden/make_engine_golden.py     # needs oracle/_ref (this container)
+    python tests/golden/make_engine_golden.py [NAME ...]   # needs oracle/_ref (this container)
 
 tests/test_engine_cli.py replays the same command against this engine's
 bin/XT_Engine and compares the output files.
@@ -61,7 +62,21 @@ def counts_multires_case():
     return p, t, a, files
 
 
-CASES = {"engine_plain": plain_case, "engine_counts_multires": counts_multires_case}
+def launcher_case():
+    """The launcher's geometry: physical lengths (length_r = 0.65 N_r,
+    length_t = 0.65 N_t, so delta_t != 1: quirk of XT_VoxUpdate.c:27,67 against
+    XT_ForwardProject.c:17), positivity off (the launcher's compile line,
+    4D_Recon_Launcher_for_Real_Data/XT_Initialize.py:257: the reference
+    binary built without POSITIVITY_CONSTRAINT), zinger correction, NHICD,
+    offset and variance estimation, 3 iterations."""
+    p = common.params(N=32, NT=4, NP=36, pitch=0.65, positivity=0, zinger=True, nhicd=True, offset=2, var=1)
+    t, a = common.views(p)
+    x, ax, y, w = common.data(p, t, a, seed=12, zfrac=0.01)
+    files = {"projection_n0.bin": y.tobytes(), "weight_n0.bin": w.tobytes()}
+    return p, t, a, files
+
+
+CASES = {"engine_plain": plain_case, "engine_counts_multires": counts_multires_case, "engine_launcher": launcher_case}
 
 
 def run(name):
@@ -74,11 +89,12 @@ def run(name):
                 fh.write(b)
         before = set(os.listdir(d))
         ins = {f: open(os.path.join(d, f), "rb").read() for f in sorted(before)}
-        r = subprocess.run([REF_ENGINE] + args, cwd=d, capture_output=True, text=True)
+        engine = REF_ENGINE if p.positivity else REF_ENGINE + "_nopos"
+        r = subprocess.run([engine] + args, cwd=d, capture_output=True, text=True)
         assert r.returncode == 0, r.stdout + r.stderr
         outs = {f: open(os.path.join(d, f), "rb").read() for f in sorted(os.listdir(d))
                 if f.endswith(".bin") and (f not in before or open(os.path.join(d, f), "rb").read() != ins.get(f))}
-    rec = {"args": np.array(args)}
+    rec = {"args": np.array(args), "positivity": np.int32(p.positivity)}
     for f, b in ins.items():
         rec["in:" + f] = np.frombuffer(b, np.uint8)
     for f, b in outs.items():
@@ -89,7 +105,7 @@ def run(name):
 def main():
     if not os.path.exists(REF_ENGINE):
         sys.exit("oracle/_ref is not built (make -C oracle needs the reference tree)")
-    for name in CASES:
+    for name in sys.argv[1:] or CASES:
         rec = run(name)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **rec)
         print("wrote", name, sorted(k for k in rec if k.startswith("out:")))

@@ -7,6 +7,9 @@ the oracle restatement (oracle/xt_oracle.c) against these files, so the pin
 holds on machines without the reference tree.
 
     python tests/golden/make_golden.py      # needs oracle/_ref (this container)
+    python tests/golden/make_golden.py NAME # one case of CASES
+    python tests/golden/make_golden.py config_c1 | config_c2_small
+                                            # the long converged runs
 
 The RNG known-answer table is read from the reference source's own comment
 (Source_Code_4D_Fast/randlib.c:69-91) and checked against the compiled
@@ -27,7 +30,9 @@ import common  # noqa: E402
 import xtg  # noqa: E402
 from oracle.oracle import Reference, ref_available  # noqa: E402
 
-REF_SRC = "/root/reference/Source_Code_4D_Fast/randlib.c"
+# the reference tree (read-only); TIMBIR_REFERENCE overrides its location
+REF_TREE = os.environ.get("TIMBIR_REFERENCE", "/root/reference")
+REF_SRC = os.path.join(REF_TREE, "Source_Code_4D_Fast", "randlib.c")
 
 CASES = {
     # name: (params kwargs, view kind, data kwargs, iterations)
@@ -39,6 +44,10 @@ CASES = {
     "timbir4d": (dict(N=16, NT=2, NP=48, n_time=3), (4, 16), dict(seed=3, moving=2), 3),
     "blocks_z": (dict(N=16, NT=8, NP=20, threads=4, nhicd=True), None, dict(seed=4), 3),
     "coarse_xy2": (dict(N=32, NT=4, NP=30, dxy=2.0, dz=2.0), None, dict(seed=5), 2),
+    # the launcher's geometry: physical lengths (delta_r = delta_t = 0.65),
+    # positivity off, zinger correction, NHICD and offset re-estimation
+    "launcher_geom": (dict(N=32, NT=4, NP=36, pitch=0.65, positivity=0, zinger=True, nhicd=True, offset=2), None,
+                      dict(seed=8, zfrac=0.01), 3),
 }
 
 
@@ -185,6 +194,44 @@ def config_c1():
     return out
 
 
+def config_c2_small(max_iters=500, stall=1e-9):
+    """The at-scale configuration's options at a size the CPU finishes: 16
+    slices of 128^2, 128 bins x 16 rows, 512 views uniform over 180 degrees,
+    30 ellipsoids, 1e4 photons/ray, 0.5 % of the sinogram entries turned into
+    zingers (+U(2, 5)), generalized-Huber zinger correction on (T = 4,
+    delta = 0.5), NHICD on, positivity on.  The FP64 reference runs from its
+    own zero start until its cost stalls (decrease over 10 iterations below
+    `stall` relative) or `max_iters`; its cost per iteration (the last is the
+    converged cost C*) and its converged object are stored."""
+    p = common.params(N=128, NT=16, NP=512, zinger=True, nhicd=True, threads=8)
+    with tempfile.TemporaryDirectory() as d:
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            t, a = common.views(p)
+            xtg.write_view_file("view_info.txt", t, a)
+            x, ax, y, w = common.data(p, t, a, seed=7, n_ell=30, mu=0.01, I0=1e4, zfrac=0.005)
+            out = dict(times=t, angles=a, y_sum=np.float64(y.astype(np.float64).sum()),
+                       w_sum=np.float64(w.astype(np.float64).sum()))
+            r = Reference(p, double=True)
+            r.set_sino(y, w)
+            r.init_error_sino()
+            r.srandom2(761521)
+            cs = [r.cost()[0]]
+            for it in range(1, max_iters + 1):
+                r.iterate(it)
+                cs.append(r.cost()[0])
+                print(f"config_c2_small iteration {it}: cost {cs[-1]!r}", flush=True)
+                if it >= 30 and cs[-11] - cs[-1] < stall * abs(cs[-1]):
+                    break
+            out["costs64"] = np.array(cs)
+            out["x_star"] = r.object().astype(np.float32)
+            r.close()
+        finally:
+            os.chdir(cwd)
+    return out
+
+
 def main():
     if not ref_available():
         sys.exit("oracle/_ref is not built (make -C oracle needs the reference tree)")
@@ -203,5 +250,9 @@ def main():
 if __name__ == "__main__":
     if sys.argv[1:] == ["config_c1"]:
         np.savez_compressed(os.path.join(HERE, "config_c1.npz"), **config_c1())
+    elif sys.argv[1:] == ["config_c2_small"]:
+        np.savez_compressed(os.path.join(HERE, "config_c2_small.npz"), **config_c2_small())
+    elif len(sys.argv) == 2 and sys.argv[1] in CASES:
+        np.savez_compressed(os.path.join(HERE, f"{sys.argv[1]}.npz"), **run_case(sys.argv[1], *CASES[sys.argv[1]]))
     else:
         main()

@@ -23,7 +23,9 @@ import common
 pytestmark = pytest.mark.gpu
 
 ENGINE = os.path.join(common.ROOT, "timbir-python_b200", "bin", "XT_Engine")
-NAMES = ["engine_plain", "engine_counts_multires"]
+# engine_launcher: the launcher's physical lengths (delta_t = 0.65) and its
+# positivity-off build
+NAMES = ["engine_plain", "engine_counts_multires", "engine_launcher"]
 
 
 def run_engine(name, tmp_path, extra):
@@ -31,8 +33,10 @@ def run_engine(name, tmp_path, extra):
     for k, v in g.items():
         if k.startswith("in:"):
             (tmp_path / k[3:]).write_bytes(v.tobytes())
-    # the reference binary was compiled with -DPOSITIVITY_CONSTRAINT
-    args = [str(s) for s in g["args"]] + ["--positivity", "1"]
+    # the reference binary's compile-time POSITIVITY_CONSTRAINT as this
+    # engine's runtime switch (older fixtures: compiled with it)
+    pos = int(g["positivity"]) if "positivity" in g else 1
+    args = [str(s) for s in g["args"]] + ["--positivity", str(pos)]
     r = subprocess.run([ENGINE] + args + extra, cwd=tmp_path, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     want = {k[4:]: np.frombuffer(v.tobytes(), np.float32) for k, v in g.items() if k.startswith("out:")}

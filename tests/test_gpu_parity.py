@@ -30,6 +30,8 @@ CASES = {
     "timbir4d": dict(N=16, NT=2, NP=48, n_time=3),
     "blocks_z": dict(N=16, NT=8, NP=20, threads=4, nhicd=True),
     "coarse_xy2": dict(N=32, NT=4, NP=30, dxy=2.0, dz=2.0),
+    # the launcher's physical lengths (delta_r = delta_t = 0.65) and positivity off
+    "launcher_geom": dict(N=32, NT=4, NP=36, pitch=0.65, positivity=0, zinger=True, nhicd=True, offset=2),
 }
 
 
@@ -83,13 +85,21 @@ def test_error_sinogram_and_cost(name):
     c.upload_object(g["x_true"])
     c.init_error_sino()
     assert np.array_equal(c.error_sino(), g["e_true"])
-    cost, fwd, prior = c.cost()
-    # the reference sums its cost in FP32 (~1e-5 relative rounding over a few
-    # thousand terms); the GPU sums in FP64
+    # the reference's cost of that e (computeCost reads the running e); it
+    # sums in FP32 (~1e-5 relative rounding over a few thousand terms), the
+    # GPU in FP64
     ref = g["cost_true"]
-    assert cost == pytest.approx(float(ref[0]), rel=1e-4)
-    assert fwd == pytest.approx(float(ref[1]), rel=1e-4)
-    assert prior == pytest.approx(float(ref[2]), rel=1e-4, abs=1e-6)
+    run = c.cost_running()
+    assert run[0] == pytest.approx(float(ref[0]), rel=1e-4)
+    assert run[1] == pytest.approx(float(ref[1]), rel=1e-4)
+    assert run[2] == pytest.approx(float(ref[2]), rel=1e-4, abs=1e-6)
+    # the recomputed FP64 cost takes e = y - A delta_t x - d, the matrix of
+    # the voxel update; the reference's projector leaves delta_t out
+    # (XT_ForwardProject.c:17), so the two agree where delta_t = 1
+    cost, fwd, prior = c.cost()
+    assert prior == pytest.approx(run[2], rel=1e-12, abs=1e-12)
+    if c.geometry().delta_t == 1.0:
+        assert cost == pytest.approx(run[0], rel=1e-6)
     # against the FP64 oracle on the same object: the GPU evaluates in FP64
     # with the FP32 build's prior constants (filter weights, sigma powers), so
     # the two agree to FP32 rounding of those constants
@@ -98,9 +108,10 @@ def test_error_sinogram_and_cost(name):
     o.set_object(g["x_true"])
     o.init_error_sino()
     assert prior == pytest.approx(o.cost()[2], rel=1e-6, abs=1e-9)
-    # the running-e cost and the FP64 resync agree with the recomputed cost
-    assert c.cost_running()[0] == pytest.approx(cost, rel=1e-6)
+    # the FP64 resync agrees with the recomputed cost, and so does the running
+    # e it leaves behind
     assert c.resync_fp64()[0] == pytest.approx(cost, rel=1e-12)
+    assert c.cost_running()[0] == pytest.approx(cost, rel=1e-6)
 
 
 @pytest.mark.parametrize("name", ["plain3d", "timbir4d", "offset_zero_mean"])
@@ -169,7 +180,8 @@ def test_nhicd_selection_bit_exact():
 @pytest.mark.parametrize("name,amode", [("plain3d", xtg.XTG_A_FP32), ("plain3d", xtg.XTG_A_TABLE32),
                                         ("timbir4d", xtg.XTG_A_FP32), ("timbir4d", xtg.XTG_A_TABLE32),
                                         ("blocks_z", xtg.XTG_A_FP32), ("coarse_xy2", xtg.XTG_A_FP32),
-                                        ("coarse_xy2", xtg.XTG_A_TABLE32), ("zinger_nhicd", xtg.XTG_A_FP32)])
+                                        ("coarse_xy2", xtg.XTG_A_TABLE32), ("zinger_nhicd", xtg.XTG_A_FP32),
+                                        ("launcher_geom", xtg.XTG_A_FP32), ("launcher_geom", xtg.XTG_A_TABLE32)])
 def test_sequential_iteration_matches_reference(name, amode):
     """Reference visiting order (same RNG draws): after iteration 1 the object
     equals the reference's up to theta summation order."""
@@ -183,7 +195,7 @@ def test_sequential_iteration_matches_reference(name, amode):
     assert np.max(np.abs(x - ref)) / scale < 1e-4
     cost = c.cost()[0]
     assert cost == pytest.approx(float(g["costs"][0][0]), rel=1e-4)
-    if name in ("zinger_nhicd",):
+    if name in ("zinger_nhicd", "launcher_geom"):
         assert np.allclose(c.offset(), g["offsets"][0], rtol=1e-3, atol=1e-5)
         assert c.variance() == pytest.approx(float(g["vars"][0]), rel=1e-4)
 
@@ -204,7 +216,9 @@ def converged_cost_fp64(name, iters=120):
                                               ("plain3d", xtg.XTG_A_TABLE32, 0), ("zinger_nhicd", xtg.XTG_A_FP32, 0),
                                               ("zinger_nhicd", xtg.XTG_A_TABLE32, 0), ("timbir4d", xtg.XTG_A_FP32, 0),
                                               ("timbir4d", xtg.XTG_A_FP16, 0), ("plain3d", xtg.XTG_A_TABLE32, 2),
-                                              ("zinger_nhicd", xtg.XTG_A_TABLE32, 1), ("blocks_z", xtg.XTG_A_FP32, 4)])
+                                              ("zinger_nhicd", xtg.XTG_A_TABLE32, 1), ("blocks_z", xtg.XTG_A_FP32, 4),
+                                              ("launcher_geom", xtg.XTG_A_TABLE32, 0),
+                                              ("launcher_geom", xtg.XTG_A_FP16, 0)])
 def test_parallel_icd_converges_to_oracle(name, amode, zslab):
     """zslab > 0 cuts every column visit into z pieces of that many slices,
     visited piece-major (the schedule large volumes use to keep e and w in L2)."""

@@ -19,6 +19,7 @@ CASES = {
     "timbir4d": (dict(N=16, NT=2, NP=48, n_time=3), (4, 16)),
     "blocks_z": (dict(N=16, NT=8, NP=20, threads=4, nhicd=True), None),
     "coarse_xy2": (dict(N=32, NT=4, NP=30, dxy=2.0, dz=2.0), None),
+    "launcher_geom": (dict(N=32, NT=4, NP=36, pitch=0.65, positivity=0, zinger=True, nhicd=True, offset=2), None),
 }
 
 

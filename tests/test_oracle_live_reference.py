@@ -2,8 +2,9 @@
 routines compiled from its sources (oracle/_ref), live, on seeded random
 geometries beyond the committed fixtures: detector sizes, view counts,
 delta_xy / delta_z of 1 and 2, rotation centres off the middle, zinger
-correction and NHICD on and off, offset re-estimation; and 4D cases of 2-3
-frames of interlaced views with moving objects.  Skipped where the
+correction and NHICD on and off, offset re-estimation; the launcher's
+physical detector pitch (delta_r = delta_t = 0.65) with positivity on and
+off; and 4D cases of 2-3 frames of interlaced views with moving objects.  Skipped where the
 reference build is absent (the committed fixtures pin the oracle there).
 
 Single-threaded, so everything is compared bit for bit: the geometry
@@ -99,6 +100,18 @@ def compare(pk, dk, interlaced, seed, tmp_path, monkeypatch):
 @pytest.mark.parametrize("seed", range(8))
 def test_oracle_matches_reference_live(seed, tmp_path, monkeypatch):
     pk, dk = random_case(seed)
+    compare(pk, dk, None, seed, tmp_path, monkeypatch)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_matches_reference_live_launcher_geometry(seed, tmp_path, monkeypatch):
+    """The launcher's geometry: physical lengths (length_r = 0.65 N_r,
+    length_t = 0.65 N_t, so delta_r = delta_t = 0.65 and the voxel update's
+    A * delta_t differs from the projector's A, XT_VoxUpdate.c:27,67 against
+    XT_ForwardProject.c:17), and positivity off in every other case (the
+    launcher's build, 4D_Recon_Launcher_for_Real_Data/XT_Initialize.py:257)."""
+    pk, dk = random_case(50 + seed)
+    pk.update(pitch=0.65, positivity=seed % 2)
     compare(pk, dk, None, seed, tmp_path, monkeypatch)
 
 

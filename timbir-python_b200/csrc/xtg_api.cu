@@ -1075,6 +1075,8 @@ __global__ void k_bin_sino(int np, int nrc, int ntc, int nrf, int ntf, int fr, i
   }
 }
 
+extern "C" int xtg_init_error_model(xtg_ctx *c);
+
 int xtg_init_object_multires(xtg_ctx *c, int32_t coarse_iters, int32_t flags) {
   if (!c || coarse_iters < 0 || (flags & ~(XTG_MULTIRES_Z | XTG_MULTIRES_BIN))) return XTG_E_ARG;
   if (!c->have_sino) {
@@ -1143,7 +1145,7 @@ int xtg_init_object_multires(xtg_ctx *c, int32_t coarse_iters, int32_t flags) {
   if (rc) return rc;
   rc = xtg_object_from_device(c, c->d_tmp);
   if (rc) return rc;
-  return xtg_init_error_sino(c);
+  return xtg_init_error_model(c);
 }
 
 int xtg_download_object(xtg_ctx *c, float *x) {
@@ -1246,6 +1248,18 @@ int xtg_init_error_sino(xtg_ctx *c) {
 
 static int finish_cost(xtg_ctx *c, double data_sum, double *cost, double *fwd, double *prior);
 
+// e for a start this library computed itself (FBP, multi-resolution, the
+// network): e = y - A delta_t x - d, the error sinogram of the matrix the
+// voxel update uses, so ICD continues from a consistent state.  With
+// delta_t = 1 that is the reference's projection (bit-exact FP32 path);
+// otherwise the FP64 pass rounded to FP32 (the reference's own projector
+// leaves out delta_t, which only its zero start makes harmless).
+__attribute__((visibility("hidden"))) int xtg_init_error_model(xtg_ctx *c) {
+  if (!c) return XTG_E_ARG;
+  if (c->g.delta_t == 1.0f) return xtg_init_error_sino(c);
+  return xtg_resync_fp64(c, nullptr, nullptr, nullptr);
+}
+
 // the FBP image into the object, leaving e stale (filtered sinogram in it):
 // for callers inside the library that replace the object again before they
 // iterate (not exported)
@@ -1264,7 +1278,7 @@ __attribute__((visibility("hidden"))) int xtg_fbp_image_only(xtg_ctx *c) {
 
 int xtg_init_object_fbp(xtg_ctx *c) {
   const int rc = xtg_fbp_image_only(c);
-  return rc ? rc : xtg_init_error_sino(c);
+  return rc ? rc : xtg_init_error_model(c);
 }
 
 int xtg_resync_fp64(xtg_ctx *c, double *cost, double *fwd, double *prior) {

@@ -46,9 +46,12 @@ __device__ __forceinline__ bool fp_col_range(const DevGeo &G, float cp, float sp
   return *klo <= *khi;
 }
 
-// MODE 0: out = A x; 1: out = e = y - A x - d (FP32, the reference's order);
-// 2: FP64 sums, out = (float)(y - A x - d), data cost into cost slots;
-// 3: FP64 data cost only.
+// MODE 0: out = A x; 1: out = e = y - A x - d (FP32, the reference's order
+// and its projector, which leaves out delta_t, XT_ForwardProject.c:17);
+// 2: FP64 sums, out = (float)(y - delta_t A x - d), data cost into cost slots;
+// 3: FP64 data cost only.  Modes 2 and 3 use A * delta_t, the matrix the
+// voxel update subtracts from e (XT_VoxUpdate.c:27, 67): the error sinogram
+// the reference carries from its zero start; with delta_t = 1 all modes agree.
 // Warp w of the CTA owns 32 consecutive detector bins of view p and keeps
 // their partial sums for 64 detector rows in shared memory (lane owns rows
 // lane and lane + 32, so the shared accesses are free of bank conflicts).  For each image row (in increasing order) the warp
@@ -161,7 +164,8 @@ __global__ void __launch_bounds__(FP_WARPS * 32) k_fp_bins(DevGeo G, FpArgs F) {
       } else if (MODE == 1) {
         F.out[o] = __fsub_rn(__fsub_rn(F.y[o], (float)sacc), F.d[od]);
       } else {
-        const double e64 = (double)F.y[o] - (double)sacc - (double)F.d[od];
+        // A * delta_t: the system matrix of the voxel update (XT_VoxUpdate.c:27, 67)
+        const double e64 = (double)F.y[o] - (double)G.delta_t * (double)sacc - (double)F.d[od];
         if (MODE == 2) F.out[o] = (float)e64;
         const double sw = e64 * sqrt((double)F.w[o]);
         if (fabs(sw) < (double)F.T)

@@ -9,6 +9,7 @@
 void xtg_set_error_text(const char *msg);
 float *xtc_net_start_buffer(xtc_net *n, size_t floats);  // cnn_net.cu
 extern "C" int xtg_fbp_image_only(xtg_ctx *c);             // xtg_api.cu
+extern "C" int xtg_init_error_model(xtg_ctx *c);           // xtg_api.cu
 
 extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coarse_iters, int32_t *used,
                                        double *cost_net, double *cost_base) {
@@ -35,19 +36,19 @@ extern "C" int xtg_init_object_learned(xtg_ctx *ctx, xtc_net *net, int32_t coars
   do {
     // the FBP image only: the multi-resolution start below recomputes e
     if ((rc = xtg_fbp_image_only(ctx)) || (rc = xtg_object_to_device(ctx, fbp))) break;
-    // the multi-resolution start (it ends with e = y - Ax - d recomputed, so
+    // the multi-resolution start (it ends with e = y - A delta_t x - d recomputed, so
     // both candidates are costed from a fresh e)
     if ((rc = xtg_init_object_multires(ctx, coarse_iters, N_z % 2 == 0 && N_z >= 16)) ||
         (rc = xtg_object_to_device(ctx, icd)) || (rc = xtg_map_cost_running(ctx, &ci, nullptr, nullptr)))
       break;
     if ((rc = xtc_net_forward(net, fbp, icd, out, N_time, N_y, N_x, N_z))) break;
-    if ((rc = xtg_object_from_device(ctx, out)) || (rc = xtg_init_error_sino(ctx)) ||
+    if ((rc = xtg_object_from_device(ctx, out)) || (rc = xtg_init_error_model(ctx)) ||
         (rc = xtg_map_cost_running(ctx, &cn, nullptr, nullptr)))
       break;
     // lower by more than the run-to-run noise of the FP64 cost sums (their
     // atomic accumulation order varies), so an unchanged image is not "better"
     use = cn < ci * (1.0 - 1e-9);
-    if (!use && ((rc = xtg_object_from_device(ctx, icd)) || (rc = xtg_init_error_sino(ctx)))) break;
+    if (!use && ((rc = xtg_object_from_device(ctx, icd)) || (rc = xtg_init_error_model(ctx)))) break;
   } while (0);
   if (rc) return rc;
   if (used) *used = use;
