@@ -224,6 +224,35 @@ def network_roofline(ctx, net, coarse_iters, reps=3):
             "frac": flops / ms / 1e9 / peak, "peak_kind": kind, "bound": "tensor"}
 
 
+def network_forward(nxy, nz, reps, weights=WEIGHTS):
+    """`--network-forward`: the warm-start network's forward pass alone (the
+    inference inside the learned start) on one volume [1][nxy][nxy][nz] of
+    seeded random images, committed weights, cuda:0; CUDA-event time per pass
+    and algorithmic TFLOP/s (2 x 27 x cin x cout per output voxel and layer)."""
+    import torch
+    net = xtg.WarmNet()
+    net.load(weights)
+    shape = (1, nxy, nxy, nz)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    f = torch.rand(shape, device="cuda", generator=g) * 0.01
+    q = f * 0.9
+    o = torch.empty(shape, device="cuda")
+    net.forward(f, q, o, shape)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.forward(f, q, o, shape)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(reps, 1)
+    vox = nxy * nxy * nz
+    flops = sum(2.0 * 27 * ci * co * vox / 8 ** lvl for ci, co, lvl in NET_LAYERS)
+    print(json.dumps({"network_forward": list(shape), "forward_ms": ms, "tflop": flops / 1e12,
+                      "tflops": flops / ms / 1e9}), flush=True)
+    net.close()
+
+
 def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, coarse_iters=30, learned=True):
     """Seconds to MAP cost <= (1 + tol) C* from four starts:
       zero     -- the reference's start, plain ICD with the benchmark's A storage;
@@ -576,10 +605,16 @@ def main():
                     help="voxels per side (= detector bins) instead of the workload's; for profiling captures")
     ap.add_argument("--zslab", type=int, default=0,
                     help="z slices per ICD work piece (0: chosen from the L2 size)")
+    ap.add_argument("--network-forward", action="store_true",
+                    help="time only the warm-start network's forward pass on [1][nxy][nxy][nz] (profiling)")
+    ap.add_argument("--nz", type=int, default=64, help="slices for --network-forward")
+    ap.add_argument("--reps", type=int, default=5, help="forward passes timed by --network-forward")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the seconds-to-converged-cost run")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.network_forward:
+        network_forward(args.nxy or 512, args.nz, args.reps)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -246,7 +246,11 @@ int xtg_update_variance(xtg_ctx *ctx);
  * The first call on a device resolves the array's device address
  * (cudaGetSymbolAddress), so make that first call before any stream capture.
  * All calls share the array: calls that overlap on the GPU (other streams,
- * other host threads) race on it and must be serialised by the caller. */
+ * other host threads) race on it and must be serialised by the caller.
+ * The resolved address is kept for the life of the process: after a
+ * cudaDeviceReset of a device, do not call this entry point on that device
+ * again.  A CUDA error already pending when it is called (from the caller's
+ * own earlier work) is reported as XTG_E_CUDA and left pending. */
 #define XTG_NOALLOC_MAX_ELEMS (1 << 20)
 #define XTG_NOALLOC_MAX_MAPS 256
 int xtg_nhicd_threshold_noalloc(const float *magmap, int32_t nmaps, int32_t ny, int32_t nx, const int32_t *kth,

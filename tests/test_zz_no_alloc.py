@@ -62,6 +62,31 @@ def test_noalloc_thresholds_match_context_entry_point_twice():
     c.close()
 
 
+def test_noalloc_selection_matches_reference_fixture():
+    """The same entry point against the reference's own NHICD selection
+    (tests/golden/nhicd_select.npz, VSC_based_Voxel_Line_Select with ties):
+    the columns above the threshold are exactly the reference's lists."""
+    import torch
+
+    g = dict(np.load(f"{common.GOLDEN}/nhicd_select.npz"))
+    nt, nzb, ny, nx = g["map"].shape
+    nmaps = nt * nzb
+    kth = np.array([ny * nx - u // 10 for u in g["usn"]], np.int32)
+    lib = xtg.gpu_lib()
+    d_map = torch.from_numpy(g["map"]).cuda()
+    d_thr = torch.zeros((nmaps,), dtype=torch.float32, device="cuda")
+    d_sel = torch.zeros((nmaps * ny * nx,), dtype=torch.uint8, device="cuda")
+    rc = lib.xtg_nhicd_threshold_noalloc(_ptr(d_map), nmaps, ny, nx, kth.ctypes.data_as(C.c_void_p), _ptr(d_thr),
+                                         _ptr(d_sel), None)
+    assert rc == 0, lib.xtg_last_error()
+    sel = d_sel.cpu().numpy().reshape(nmaps, ny, nx)
+    for s in range(nmaps):
+        want = np.zeros((ny, nx), np.uint8)
+        n = int(g["nn"][s])
+        want[g["ys"][s, :n], g["xs"][s, :n]] = 1
+        assert np.array_equal(sel[s], want), s
+
+
 def test_noalloc_rejects_oversized_input():
     import torch
 

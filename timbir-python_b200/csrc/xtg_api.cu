@@ -2090,6 +2090,14 @@ extern "C" int xtg_nhicd_threshold_noalloc(const float *magmap, int32_t nmaps, i
     }
     r.k[s] = kth[s];
   }
+  // an error left by the caller's own earlier work is reported as such and
+  // left pending for the caller, not taken for one of the launches below
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    set_err("xtg_nhicd_threshold_noalloc: a CUDA error from earlier work is pending: %s",
+            cudaGetErrorString(pending));
+    return XTG_E_CUDA;
+  }
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 256) {
@@ -2109,10 +2117,15 @@ extern "C" int xtg_nhicd_threshold_noalloc(const float *magmap, int32_t nmaps, i
   int *ranks = reinterpret_cast<int *>(filt + XTG_NOALLOC_MAX_ELEMS);
   // every value read below is written first in this call: no clearing needed
   k_noalloc_put_ranks<<<1, 256, 0, st>>>(r, nmaps, ranks);
+  CK(cudaGetLastError());
   const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, 4096);
   k_vsc_filter<<<grid, 256, 0, st>>>(nmaps, ny, nx, magmap, filt);
-  k_radix_select<<<nmaps, 1024, 0, st>>>(filt, (int)plane, ranks, thresholds);
-  if (select) k_noalloc_select<<<grid, 256, 0, st>>>(n, (int)plane, filt, thresholds, select);
   CK(cudaGetLastError());
+  k_radix_select<<<nmaps, 1024, 0, st>>>(filt, (int)plane, ranks, thresholds);
+  CK(cudaGetLastError());
+  if (select) {
+    k_noalloc_select<<<grid, 256, 0, st>>>(n, (int)plane, filt, thresholds, select);
+    CK(cudaGetLastError());
+  }
   return 0;
 }

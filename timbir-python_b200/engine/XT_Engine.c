@@ -51,7 +51,10 @@ static void logf_(const char *fmt, ...) {
   va_end(ap);
 }
 
-/* Read4mBin (XT_IOMisc.c:79-96), but a short read is fatal here */
+/* Read4mBin (XT_IOMisc.c:79-96): a missing file is fatal (exit status 1, as
+ * in the reference); a short read is logged with the reference's message and
+ * the run continues, the unread rest of the array left at zero (the
+ * reference continues with whatever its buffer held there). */
 static int read_bin(const char *name, float *dst, size_t n) {
   char file[512];
   snprintf(file, sizeof(file), "%s.bin", name);
@@ -64,6 +67,11 @@ static int read_bin(const char *name, float *dst, size_t n) {
   size_t got;
   if (g_dbl) {
     double *t = (double *)malloc(n * sizeof(double));
+    if (!t) {
+      fclose(fp);
+      logf_("ERROR: out of host memory reading %s\n", file);
+      return -1;
+    }
     got = fread(t, sizeof(double), n, fp);
     for (size_t i = 0; i < got; i++) dst[i] = (float)t[i];
     free(t);
@@ -73,8 +81,8 @@ static int read_bin(const char *name, float *dst, size_t n) {
   fclose(fp);
   if (got != n) {
     logf_("ERROR: Number of elements read does not match required, required = %zu, read = %zu\n", n, got);
-    fprintf(stderr, "ERROR: %s: read %zu of %zu elements\n", file, got, n);
-    return -1;
+    fprintf(stderr, "WARNING: %s: read %zu of %zu elements; the rest is taken as zero\n", file, got, n);
+    memset(dst + got, 0, (n - got) * sizeof(float));
   }
   return 0;
 }
@@ -113,60 +121,6 @@ static int write_scalar(const char *name, double v, const char *mode) {
   return write_bin(name, &f, 1, mode);
 }
 
-/* bilinear x2 in x and y of [nz][ny][nx] (edge samples copied, interior 3:1
- * weights), upsample_object_bilinear_2D, XT_ICD_update.c:354-386 */
-static void up_xy(const float *in, float *out, int nz, int ny, int nx) {
-  float *buf = (float *)malloc(sizeof(float) * (size_t)ny * 2 * nx);
-  for (int s = 0; s < nz; s++) {
-    const float *I = in + (size_t)s * ny * nx;
-    float *O = out + (size_t)s * 4 * ny * nx;
-    for (int j = 0; j < ny; j++) {
-      const float *a = I + (size_t)j * nx;
-      float *b = buf + (size_t)j * 2 * nx;
-      b[0] = a[0];
-      b[1] = (float)((3.0 * a[0] + a[1]) / 4.0);
-      b[2 * nx - 1] = a[nx - 1];
-      b[2 * nx - 2] = (float)((a[nx - 2] + 3.0 * a[nx - 1]) / 4.0);
-      for (int k = 1; k < nx - 1; k++) {
-        b[2 * k] = (float)((a[k - 1] + 3.0 * a[k]) / 4.0);
-        b[2 * k + 1] = (float)((3.0 * a[k] + a[k + 1]) / 4.0);
-      }
-    }
-    const size_t w = 2 * (size_t)nx;
-    for (size_t k = 0; k < w; k++) {
-      O[k] = buf[k];
-      O[w + k] = (float)((3.0 * buf[k] + buf[w + k]) / 4.0);
-      O[(2 * (size_t)ny - 1) * w + k] = buf[(size_t)(ny - 1) * w + k];
-      O[(2 * (size_t)ny - 2) * w + k] = (float)((buf[(size_t)(ny - 2) * w + k] + 3.0 * buf[(size_t)(ny - 1) * w + k]) / 4.0);
-    }
-    for (int j = 1; j < ny - 1; j++)
-      for (size_t k = 0; k < w; k++) {
-        O[(2 * (size_t)j) * w + k] = (float)((buf[(size_t)(j - 1) * w + k] + 3.0 * buf[(size_t)j * w + k]) / 4.0);
-        O[(2 * (size_t)j + 1) * w + k] = (float)((3 * buf[(size_t)j * w + k] + buf[(size_t)(j + 1) * w + k]) / 4.0);
-      }
-  }
-  free(buf);
-}
-
-/* x2 in x, y and z, upsample_object_bilinear_3D, XT_ICD_update.c:388-436 */
-static void up_xyz(const float *in, float *out, int nz, int ny, int nx) {
-  const size_t pl = (size_t)4 * ny * nx;
-  float *b3 = (float *)malloc(sizeof(float) * (size_t)nz * pl);
-  up_xy(in, b3, nz, ny, nx);
-  for (size_t q = 0; q < pl; q++) {
-    out[q] = b3[q];
-    out[pl + q] = (float)((3.0 * b3[q] + b3[pl + q]) / 4.0);
-    out[(size_t)(2 * nz - 1) * pl + q] = b3[(size_t)(nz - 1) * pl + q];
-    out[(size_t)(2 * nz - 2) * pl + q] = (float)((3.0 * b3[(size_t)(nz - 1) * pl + q] + b3[(size_t)(nz - 2) * pl + q]) / 4.0);
-  }
-  for (int s = 1; s < nz - 1; s++)
-    for (size_t q = 0; q < pl; q++) {
-      out[(size_t)(2 * s) * pl + q] = (float)((b3[(size_t)(s - 1) * pl + q] + 3.0 * b3[(size_t)s * pl + q]) / 4.0);
-      out[(size_t)(2 * s + 1) * pl + q] = (float)((3.0 * b3[(size_t)s * pl + q] + b3[(size_t)(s + 1) * pl + q]) / 4.0);
-    }
-  free(b3);
-}
-
 static int write_outputs(xtg_ctx *ctx, const int32_t *dims) {
   const int N_x = dims[0], N_y = dims[1], N_z = dims[2], N_time = dims[3], N_r = dims[4], N_t = dims[5];
   const size_t vol = (size_t)N_z * N_y * N_x;
@@ -188,6 +142,102 @@ static int write_outputs(xtg_ctx *ctx, const int32_t *dims) {
   rc |= write_bin("proj_offset_n0", d, (size_t)N_r * N_t, "wb");
   free(x);
   free(d);
+  return rc;
+}
+
+/* The sinogram and the offset d (genSinogram_fromBin / _subsampleCounts,
+ * XT_genSinogram.c:264-374; the offset of XT_Init.c:340-366, replicated from
+ * the coarser stage's detector with initICD 2 / 3 and counts ingest). */
+static int load_sinogram(xtg_ctx *ctx, const xt_params *P, const int32_t *dims) {
+  const int N_r = dims[4], N_t = dims[5], N_p = dims[6];
+  const size_t ns = (size_t)N_p * N_r * N_t, nrt = (size_t)N_r * N_t;
+  float *d = NULL, *t = NULL, *y = NULL, *w = NULL;
+  int rc = -1;
+  if (P->updateProjOffset == 1 || P->updateProjOffset == 3) {
+    d = (float *)calloc(nrt, sizeof(float));
+    if (!d) goto out;
+    int pxy = 1, pz = 1;
+    if (P->initICD == 3) pxy = pz = 2;
+    if (P->initICD == 2) pxy = 2;
+    if (P->sinobin == 3 && (pxy > 1 || pz > 1)) {
+      t = (float *)calloc((size_t)(N_r / pxy) * (N_t / pz), sizeof(float));
+      if (!t || read_bin("proj_offset_n0", t, (size_t)(N_r / pxy) * (N_t / pz))) goto out;
+      for (int i = 0; i < N_r / pxy; i++)
+        for (int j = 0; j < N_t / pz; j++)
+          for (int a = 0; a < pxy; a++)
+            for (int b = 0; b < pz; b++) d[(size_t)(i * pxy + a) * N_t + j * pz + b] = t[(size_t)i * (N_t / pz) + j];
+    } else if (read_bin("proj_offset_n0", d, nrt)) {
+      goto out;
+    }
+  }
+  if (P->sinobin == 1) {
+    y = (float *)malloc(ns * sizeof(float));
+    w = (float *)malloc(ns * sizeof(float));
+    if (!y || !w || read_bin("projection_n0", y, ns) || read_bin("weight_n0", w, ns)) goto out;
+    rc = xtg_upload_sino(ctx, y, w, d);
+  } else {
+    const int mxy = (int)P->delta_xy, mz = (int)P->delta_z;
+    const size_t nb = (size_t)N_r * mxy * N_t * mz;
+    y = (float *)malloc(nb * sizeof(float));        /* bright */
+    w = (float *)malloc(nb * N_p * sizeof(float));  /* counts */
+    if (!y || !w || read_bin("bright_n0", y, nb) || read_bin("weight_n0", w, nb * N_p)) goto out;
+    const char *bh = getenv("XT_BH_QUAD_COEF");
+    rc = xtg_upload_counts(ctx, y, w, bh ? atof(bh) : 0.0, d);
+  }
+  if (rc) logf_("ERROR: %s\n", xtg_last_error());
+out:
+  if (rc && !y) logf_("ERROR: out of host memory or unreadable input\n");
+  free(d);
+  free(t);
+  free(y);
+  free(w);
+  return rc;
+}
+
+/* initObject (XT_ICD_update.c:443-536) with initICD 1 / 2 / 3: the object of
+ * this or the coarser stage, upsampled on the GPU with the reference's
+ * bilinear schemes (upsample_object_bilinear_2D / _3D, XT_ICD_update.c:354-436),
+ * and with --initMagUpMap the magnitude-update map (upsample_bilinear_2D of
+ * each (frame, z-block) plane, XT_ICD_update.c:318-352). */
+static int load_object(xtg_ctx *ctx, const xt_params *P, const int32_t *dims) {
+  const int N_x = dims[0], N_y = dims[1], N_z = dims[2], N_time = dims[3], nzb = dims[7];
+  const size_t vol = (size_t)N_z * N_y * N_x, nmag = (size_t)N_time * nzb * N_y * N_x;
+  const int sxy = P->initICD >= 2 ? 2 : 1, sz = P->initICD == 3 ? 2 : 1;
+  const size_t cvol = (size_t)(N_z / sz) * (N_y / sxy) * (N_x / sxy);
+  float *x = (float *)calloc(vol * N_time, sizeof(float));
+  float *t = sxy > 1 ? (float *)calloc(cvol * N_time, sizeof(float)) : NULL;
+  float *m = NULL;
+  int rc = -1;
+  char name[256];
+  if (!x || (sxy > 1 && !t)) goto out;
+  for (int i = 0; i < N_time; i++) {
+    snprintf(name, sizeof(name), "object_n0_time_%d", i);
+    if (read_bin(name, sxy > 1 ? t + (size_t)i * cvol : x + (size_t)i * vol, sxy > 1 ? cvol : vol)) goto out;
+  }
+  if (sxy > 1 && xtg_upsample(ctx, t, x, N_time, N_z / sz, N_y / 2, N_x / 2, sz > 1)) goto gpu_err;
+  if (xtg_upload_object(ctx, x)) goto gpu_err;
+  if (P->initMagUpMap) {
+    m = (float *)calloc(nmag, sizeof(float));
+    if (!m) goto out;
+    if (P->initICD == 1) {
+      if (read_bin("mag_update_map_n0", m, nmag)) goto out;
+    } else {
+      const size_t half = (size_t)N_time * nzb * (N_y / 2) * (N_x / 2);
+      free(t);
+      t = (float *)calloc(half, sizeof(float));
+      if (!t || read_bin("mag_update_map_n0", t, half)) goto out;
+      if (xtg_upsample(ctx, t, m, N_time * nzb, 1, N_y / 2, N_x / 2, 0)) goto gpu_err;
+    }
+    if (xtg_set_magmap(ctx, m)) goto gpu_err;
+  }
+  rc = 0;
+  goto out;
+gpu_err:
+  logf_("ERROR: %s\n", xtg_last_error());
+out:
+  free(x);
+  free(t);
+  free(m);
   return rc;
 }
 
@@ -242,6 +292,16 @@ int main(int argc, char **argv) {
   if (nv < 0) {
     logf_("%s\n", err);
     fprintf(stderr, "%s\n", err);
+    if (g_log) fclose(g_log);
+    return 1;
+  }
+  /* initSparseAnglesfrmFile's count check, XT_Init.c:158-161 */
+  if (nv != P.num_projections) {
+    logf_("ERROR: Number of projections read is %d and expected is %d\n", nv, P.num_projections);
+    fprintf(stderr, "ERROR: view_info.txt holds %d views, --num_projections is %d\n", nv, P.num_projections);
+    free(times);
+    free(angles);
+    if (g_log) fclose(g_log);
     return 1;
   }
   xtg_ctx *ctx = NULL;
@@ -257,106 +317,25 @@ int main(int argc, char **argv) {
                        O.columns, O.seed);
   if (rc) {
     logf_("ERROR: %s\n", xtg_last_error());
-    return 1;
+    goto fail;
   }
   int32_t dims[11];
   xtg_dims(ctx, dims);
-  const int N_x = dims[0], N_y = dims[1], N_z = dims[2], N_time = dims[3], N_r = dims[4], N_t = dims[5];
-  const int N_p = dims[6], nzb = dims[7];
+  const int N_x = dims[0], N_y = dims[1], N_z = dims[2], N_time = dims[3], nzb = dims[7];
   xt_geom G;
   xtg_geometry(ctx, &G);
   logf_("initStructures: Number of z blocks is %d\n", nzb);
-  const size_t ns = (size_t)N_p * N_r * N_t, nrt = (size_t)N_r * N_t;
 
   /* sinogram (genSinogram_fromBin / genSinogram_subsampleCounts) and offset */
-  float *d = NULL;
-  if (P.updateProjOffset == 1 || P.updateProjOffset == 3) {
-    d = (float *)calloc(nrt, sizeof(float));
-    int pxy = 1, pz = 1; /* offset of the coarser stage replicated, XT_Init.c:340-366 */
-    if (P.initICD == 3) pxy = pz = 2;
-    if (P.initICD == 2) pxy = 2;
-    if (P.sinobin == 3 && (pxy > 1 || pz > 1)) {
-      float *t = (float *)calloc((size_t)(N_r / pxy) * (N_t / pz), sizeof(float));
-      if (read_bin("proj_offset_n0", t, (size_t)(N_r / pxy) * (N_t / pz))) return 1;
-      for (int i = 0; i < N_r / pxy; i++)
-        for (int j = 0; j < N_t / pz; j++)
-          for (int a = 0; a < pxy; a++)
-            for (int b = 0; b < pz; b++) d[(size_t)(i * pxy + a) * N_t + j * pz + b] = t[(size_t)i * (N_t / pz) + j];
-      free(t);
-    } else if (read_bin("proj_offset_n0", d, nrt)) {
-      return 1;
-    }
-  }
-  if (P.sinobin == 1) {
-    float *y = (float *)malloc(ns * sizeof(float)), *w = (float *)malloc(ns * sizeof(float));
-    if (!y || !w || read_bin("projection_n0", y, ns) || read_bin("weight_n0", w, ns)) return 1;
-    rc = xtg_upload_sino(ctx, y, w, d);
-    free(y);
-    free(w);
-  } else {
-    const int mxy = (int)P.delta_xy, mz = (int)P.delta_z;
-    const size_t nb = (size_t)N_r * mxy * N_t * mz;
-    float *b = (float *)malloc(nb * sizeof(float)), *cts = (float *)malloc(nb * N_p * sizeof(float));
-    if (!b || !cts || read_bin("bright_n0", b, nb) || read_bin("weight_n0", cts, nb * N_p)) return 1;
-    const char *bh = getenv("XT_BH_QUAD_COEF");
-    rc = xtg_upload_counts(ctx, b, cts, bh ? atof(bh) : 0.0, d);
-    free(b);
-    free(cts);
-  }
-  free(d);
-  if (rc) {
-    logf_("ERROR: %s\n", xtg_last_error());
-    return 1;
-  }
+  if (load_sinogram(ctx, &P, dims)) goto fail;
   if (P.dont_reconstruct) {
     logf_("XT_Engine: --dont_reconstruct given, no reconstruction\n");
     xtg_destroy(ctx);
+    if (g_log) fclose(g_log);
     return 0;
   }
-
-  /* initObject (XT_ICD_update.c:443-536) */
-  const size_t vol = (size_t)N_z * N_y * N_x, nmag = (size_t)N_time * nzb * N_y * N_x;
-  if (P.initICD >= 1) {
-    float *x = (float *)calloc(vol * N_time, sizeof(float));
-    char name[256];
-    for (int i = 0; i < N_time; i++) {
-      snprintf(name, sizeof(name), "object_n0_time_%d", i);
-      if (P.initICD == 1) {
-        if (read_bin(name, x + (size_t)i * vol, vol)) return 1;
-      } else if (P.initICD == 2) {
-        float *t = (float *)malloc(sizeof(float) * (size_t)N_z * (N_y / 2) * (N_x / 2));
-        if (read_bin(name, t, (size_t)N_z * (N_y / 2) * (N_x / 2))) return 1;
-        up_xy(t, x + (size_t)i * vol, N_z, N_y / 2, N_x / 2);
-        free(t);
-      } else {
-        float *t = (float *)malloc(sizeof(float) * (size_t)(N_z / 2) * (N_y / 2) * (N_x / 2));
-        if (read_bin(name, t, (size_t)(N_z / 2) * (N_y / 2) * (N_x / 2))) return 1;
-        up_xyz(t, x + (size_t)i * vol, N_z / 2, N_y / 2, N_x / 2);
-        free(t);
-      }
-    }
-    rc = xtg_upload_object(ctx, x);
-    free(x);
-    if (rc) {
-      logf_("ERROR: %s\n", xtg_last_error());
-      return 1;
-    }
-    if (P.initMagUpMap) {
-      float *m = (float *)calloc(nmag, sizeof(float));
-      if (P.initICD == 1) {
-        if (read_bin("mag_update_map_n0", m, nmag)) return 1;
-      } else {
-        /* upsample_bilinear_2D of every (frame, block) plane, XT_ICD_update.c:318-352 */
-        const size_t half = (size_t)N_time * nzb * (N_y / 2) * (N_x / 2);
-        float *t = (float *)malloc(sizeof(float) * half);
-        if (read_bin("mag_update_map_n0", t, half)) return 1;
-        up_xy(t, m, N_time * nzb, N_y / 2, N_x / 2);
-        free(t);
-      }
-      xtg_set_magmap(ctx, m);
-      free(m);
-    }
-  }
+  const size_t nmag = (size_t)N_time * nzb * N_y * N_x;
+  if (P.initICD >= 1 && load_object(ctx, &P, dims)) goto fail;
 
   /* e = y - A x - d, then the cost before ICD (XT_ICD_update.c:998-1007);
    * with initICD 0 the zero start can be replaced by the learned, the
@@ -381,12 +360,12 @@ int main(int argc, char **argv) {
   }
   if (rc) {
     logf_("ERROR: %s\n", xtg_last_error());
-    return 1;
+    goto fail;
   }
   double cost = 0, fwd = 0, prior = 0;
   if ((rc = xtg_map_cost_fp64(ctx, &cost, &fwd, &prior))) {
     logf_("ERROR: %s\n", xtg_last_error());
-    return 1;
+    goto fail;
   }
   logf_("costCompute: forward cost=%f\ncostCompute: prior cost =%f\n", fwd, prior);
   logf_("-------------ICD_BackProject: ICD Iter=Before ICD, cost=%f------------\n", cost);
@@ -400,22 +379,21 @@ int main(int argc, char **argv) {
     if ((rc = xtg_icd_iteration(ctx, Iter, &st))) {
       logf_("ERROR: %s\n", xtg_last_error());
       fprintf(stderr, "ERROR: %s\n", xtg_last_error());
-      xtg_destroy(ctx);
-      return 1;
+      goto fail;
     }
     vox_updates += st.voxel_updates;
     logf_("updateVoxelsTimeSlices: Average voxel update over all voxels is %f, total voxels is %f\n",
           st.total_pix > 0 ? st.mag_sum / st.total_pix : 0.0, st.total_pix);
     logf_("updateVoxelsTimeSlices: Zero count is %lld\n", (long long)st.zero_skipped);
     logf_("updateVoxelsTimeSlices: percentage change in average magnitude is %f\n", st.avg_update_pct);
-    if (P.WritePerIter && write_outputs(ctx, dims)) return 1;
+    if (P.WritePerIter && write_outputs(ctx, dims)) goto fail;
     if (O.resync_every > 0 && Iter % O.resync_every == 0)
       rc = xtg_resync_fp64(ctx, &cost, &fwd, &prior);
     else
       rc = xtg_map_cost_running(ctx, &cost, &fwd, &prior);
     if (rc) {
       logf_("ERROR: %s\n", xtg_last_error());
-      return 1;
+      goto fail;
     }
     double var = 0;
     xtg_get_variance(ctx, &var);
@@ -441,10 +419,13 @@ int main(int argc, char **argv) {
   logf_("ICD_BackProject: The estimated variance is %f\n", var);
   write_scalar("variance_estimate_n0", var, "wb");
   float *m = (float *)malloc(sizeof(float) * nmag);
-  xtg_get_magmap(ctx, m);
-  write_bin("mag_update_map_n0", m, nmag, "wb");
+  if (!m || xtg_get_magmap(ctx, m) || write_bin("mag_update_map_n0", m, nmag, "wb")) {
+    logf_("ERROR: writing mag_update_map_n0.bin failed\n");
+    free(m);
+    goto fail;
+  }
   free(m);
-  if (write_outputs(ctx, dims)) return 1;
+  if (write_outputs(ctx, dims)) goto fail;
   const double t_end = now_s();
   logf_("XT_Engine: done, %d iterations, %lld voxel updates, ICD %.3f s, total %.3f s\n",
         Iter > P.iter ? P.iter : Iter, vox_updates, t_end - t_icd, t_end - t_start);
@@ -453,4 +434,8 @@ int main(int argc, char **argv) {
   if (g_log) fclose(g_log);
   (void)G;
   return 0;
+fail:
+  xtg_destroy(ctx);
+  if (g_log) fclose(g_log);
+  return 1;
 }
