@@ -290,8 +290,12 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     x_star = ctx.object()
     x_scale = float(np.abs(x_star).max()) or 1.0
     out = {"c_star": c_star, "c_star_iterations": len(hist), "tol": tol,
-           "c_star_source": "this engine from the FBP start run to a stall (FP64 resync cost); at test sizes "
-                            "the parallel schedule reaches the FP64 CPU oracle's converged cost"}
+           "c_star_source": "this engine from the FBP start run until its FP64 cost stalls; the MAP cost of "
+                            "that object is re-evaluated on the host in c_star_check (the oracle with the GPU's "
+                            "arithmetic, and the reference's FP64 build's arithmetic).  With the same options "
+                            "at 128^2 x 16 / 512 views the parallel schedule reaches the reference FP64 engine's "
+                            "own converged cost (tests/test_config_c2_pinned.py)",
+           "_x_star": x_star}
     net = None
     if learned and os.path.exists(WEIGHTS) and all(d % 8 == 0 for d in (ctx.N_x, ctx.N_y, ctx.N_z)):
         net = xtg.WarmNet()
@@ -495,21 +499,204 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    x_star = None
     if not args.no_converge and world == 1:
         # a single-GPU metric: with N replicas every rank would repeat it.
         # The committed warm-start weights were trained for the plain-3D geometry
         line["time_to_cost"] = converge(ctx, args.amode, learned=args.workload == "plain3d" and not args.nxy)
+        x_star = line["time_to_cost"].pop("_x_star")
+        # the reference's CPU-runnable configuration, to its own FP64 converged cost
+        line["time_to_cost_config1"] = config1_gpu(args.amode)
+    ctx.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
+        if x_star is not None:
+            line["time_to_cost"]["c_star_check"] = c_star_check(p, t, a, y, wt, x_star,
+                                                                line["time_to_cost"]["c_star"])
+    if world == 1 and args.workload == "plain3d" and not args.nxy and not args.no_other:
+        line["other_workloads"] = {name: other_workload(name, args) for name in ("timbir4d", "timbir4d_large")}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
+# the reference's CPU-runnable configuration (4 slices of 128^2, 128 bins,
+# 180 views at i degrees, 10 ellipsoids U(0, 0.01), 2e4 photons/ray, no zinger
+# correction, no NHICD, positivity on) and its converged cost: the reference's
+# -DREAL_IS_DOUBLE build run 150 iterations from zero
+# (tests/golden/config_c1.npz, made by tests/golden/make_golden.py)
+C1_FIXTURE = os.path.join(ROOT, "tests", "golden", "config_c1.npz")
+
+
+def config1_case():
+    p = xtg.Params(p=1.2, sigma_s=200000.0, sigma_t=200000.0, c_s=0.01, c_t=0.01, delta_xy=1.0, delta_z=1.0,
+                   length_r=128.0, length_t=4.0, rotation_center=64.0, alpha=1.0, Rtime0=0.0, Rtime_delta=180.0,
+                   radius_obj=128.0, zingerT=100000.0, zingerDel=0.0, iter=20, Rtime_num=1, num_projections=180,
+                   N_r=128, N_t=4, num_threads=1, positivity=1, no_NHICD=1)
+    t, a = xtg.round_views(*xtg.views_uniform(180))
+    x = xtg.phantom((1, 4, 128, 128), 10, 0.01, 1)
+    y, w = xtg.measure(xtg.forward_cpu(p, t, a, x), 2e4, 101)
+    g = np.load(C1_FIXTURE)
+    # the seeded generator reproduces the inputs the reference ran on
+    assert abs(y.astype(np.float64).sum() / float(g["y_sum"]) - 1) < 1e-12
+    assert abs(w.astype(np.float64).sum() / float(g["w_sum"]) - 1) < 1e-12
+    return p, t, a, y, w, float(g["costs64"][-1])
+
+
+def config1_gpu(amode, tol=1e-4, resync_every=10):
+    """Seconds from the zero start to MAP cost <= (1 + tol) C* on configuration
+    1 (wall clock, e = y - Ax - d and the cost tests included; the A storage
+    is built beforehand, like the reference's tables).  C* is the reference's
+    own FP64 converged cost; its own time for the same run is the reference
+    arm's time_to_cost_config1."""
+    import torch
+    p, t, a, y, w, c_star = config1_case()
+    c = xtg.Context(p, t, a)
+    c.set_options(a_mode=AMODES[amode])
+    c.upload_sino(y, w)
+    zero = np.zeros(c.obj_shape, np.float32)
+    c.upload_object(zero)
+    c.iteration(1)
+    c.upload_object(zero)
+    torch.cuda.synchronize()
+    target = c_star * (1 + tol)
+    t0 = time.perf_counter()
+    c.init_error_sino()
+    it, cost = 0, float("inf")
+    while it < 200:
+        it += 1
+        c.iteration(it)
+        cost = c.cost_running()[0]
+        if cost <= target or it % resync_every == 0:
+            cost = c.resync_fp64()[0]
+            if cost <= target:
+                break
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    c.close()
+    return {"workload": "config1_128x128x4_180views", "s": secs if cost <= target else None, "iterations": it,
+            "cost": cost, "c_star": c_star, "tol": tol, "a_mode": amode,
+            "c_star_source": "the reference's -DREAL_IS_DOUBLE engine, 150 iterations from zero "
+                             "(tests/golden/config_c1.npz)"}
+
+
+def config1_reference(tol=1e-4, threads=None):
+    """The reference engine's own routines (oracle/_ref, its default FP32
+    build, OpenMP on every host core) on configuration 1 from its zero start:
+    seconds until its object's MAP cost is <= (1 + tol) C*.  Timed: e = y - Ax
+    and per iteration updateVoxelsTimeSlices plus computeCost (its cost build
+    evaluates the cost every iteration).  Not timed: the judge, an FP64
+    evaluation of each iteration's object (the reference's own FP32 cost sums
+    in float and reads ~3e-5 low here, so it would stop early)."""
+    from oracle.oracle import Oracle, Reference
+    p, t, a, y, w, c_star = config1_case()
+    p.num_threads = threads or os.cpu_count()
+    judge = Oracle(p, t, a)
+    judge.set_sino(y, w)
+    cwd = os.getcwd()
+    d = tempfile.mkdtemp()
+    os.chdir(d)
+    try:
+        xtg.write_view_file("view_info.txt", t, a)
+        r = Reference(p)
+        r.set_sino(y, w)
+        r.srandom2(761521)
+        target = c_star * (1 + tol)
+        t0 = time.perf_counter()
+        r.init_error_sino()
+        r.cost()
+        secs = time.perf_counter() - t0
+        cost, it = float("inf"), 0
+        while it < 200 and cost > target:
+            it += 1
+            t0 = time.perf_counter()
+            r.iterate(it)
+            r.cost()
+            secs += time.perf_counter() - t0
+            judge.set_object(r.object())
+            cost = judge.map_cost_fp64()[0]
+        r.close()
+    finally:
+        os.chdir(cwd)
+        judge.close()
+    return {"workload": "config1_128x128x4_180views", "s": secs if cost <= target else None, "iterations": it,
+            "cost": cost, "c_star": c_star, "tol": tol, "threads": p.num_threads,
+            "judge": "MAP cost of each iteration's object with FP64 sums (not timed)",
+            "note": "the reference runs N_time x num_z_blocks / 2 = 2 tasks at once on 4 slices "
+                    "(XT_Init.c:396-400, XT_ICD_update.c:800-801)"}
+
+
+def c_star_check(p, t, a, y, w, x_star, c_star):
+    """The host re-evaluates the MAP cost of the C* object (part of the CPU
+    leg; the oracle is the checker here): with the GPU's arithmetic (FP32 A
+    and constants of the reference's default build, FP64 sums) and with the
+    reference's -DREAL_IS_DOUBLE arithmetic."""
+    from oracle.oracle import Oracle
+    out = {}
+    for double, key in ((False, "oracle_gpu_arithmetic"), (True, "oracle_reference_fp64_build")):
+        t0 = time.perf_counter()
+        o = Oracle(p, t, a, double=double)
+        o.set_sino(y, w)
+        o.set_object(x_star)
+        v = o.map_cost_fp64()[0]
+        o.close()
+        out[key] = {"cost": v, "rel_diff": v / c_star - 1.0, "s": time.perf_counter() - t0}
+    return out
+
+
+def other_workload(name, args, steps=None):
+    """Throughput (and for the 4D workload seconds to cost) of the other
+    configurations, measured after the headline one."""
+    import torch
+    w = dict(WORKLOADS[name])
+    p, t, a, x_true, y, wt = make_data(w)
+    ctx = xtg.Context(p, t, a)
+    ctx.set_options(a_mode=xtg.XTG_A_AUTO)
+    ctx.upload_sino(y, wt)
+    ctx.init_error_sino()
+    big = name == "timbir4d_large"
+    warm, steps = (1, 2) if big else (3, 10)
+    it = 0
+    for _ in range(warm):
+        it += 1
+        ctx.iteration(it)
+    torch.cuda.synchronize()
+    ms, upd, kms, n_icd = 0.0, 0, 0.0, 0
+    for _ in range(steps):
+        it += 1
+        st = ctx.iteration(it)
+        ms += st.ms
+        upd += st.voxel_updates
+        k_ms, _, k_n = ctx.last_kernel_time()
+        kms += k_ms
+        n_icd += k_n
+    nnz = nnz_per_column(ctx, p, t, a)
+    amode = {xtg.XTG_A_FP32: "fp32", xtg.XTG_A_TABLE32: "table32", xtg.XTG_A_FP16: "fp16"}[ctx.a_mode_used()]
+    b_upd = nnz * ctx.zovl * 12.0 + nnz * A_BYTES[amode] / ctx.N_z
+    peak, kind = peaks()
+    achieved = upd * b_upd / (kms / 1e3) / 1e9 if kms > 0 else 0.0
+    out = {"config": base_config(w, amode), "value": upd / (ms / 1e3), "unit": "voxel-updates/s",
+           "ms_per_step": ms / steps, "steps": steps, "warmup": warm,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "bytes_per_voxel_update": b_upd, "nnz_per_column": nnz, "kernel_ms_per_step": kms / steps,
+                        "icd_launches_per_step": n_icd / steps, "peak_kind": peak_kind_note(kind)}}
+    if not big and not args.no_converge:
+        out["time_to_cost"] = converge(ctx, amode, learned=False)
+        out["time_to_cost"].pop("_x_star")
+        out["time_to_cost"]["learned"] = "not run: the committed network was trained for the plain-3D geometry"
+    elif big:
+        out["time_to_cost"] = ("not run: its converged cost needs a run to a stall of several hundred 4.7 s "
+                               "iterations, beyond the benchmark's time")
+    ctx.close()
+    return out
+
+
 def peak_kind_note(kind):
     return f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else "fallback 6.65 TB/s"
+
+
+_SAMPLE_DATA = {}
 
 
 def ref_sample_run(w, iters=1, threads=None):
@@ -521,7 +708,11 @@ def ref_sample_run(w, iters=1, threads=None):
         return None
     threads = threads or os.cpu_count()
     radius = w["N"] / 8.0  # central disk: about 1/20 of the columns
-    p, t, a, x_true, y, wt = make_data(w)
+    key = json.dumps(w, sort_keys=True)
+    if key not in _SAMPLE_DATA:  # the same seeded data for every step
+        _SAMPLE_DATA[key] = make_data(w)
+    p, t, a, x_true, y, wt = _SAMPLE_DATA[key]
+    p = xtg.Params(**{k: getattr(p, k) for k in p.__dataclass_fields__})
     p.radius_obj = radius
     p.num_threads = threads
     cwd = os.getcwd()
@@ -577,6 +768,7 @@ def run_reference(args):
             vals.append(v)
             tot += dt
     value = float(np.mean(vals))
+    c1 = config1_reference()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -586,7 +778,8 @@ def run_reference(args):
                            parallelism="cpu"),
             "cpu_baseline": {"value": value, "unit": "voxel-updates/s", "cores": thr, "kind": "reference",
                              "sample": "one reference iteration per step on the central-disk sample"},
-            "e2e": {"value": value, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "time_to_cost_config1": c1}
     print(json.dumps(line), flush=True)
 
 
@@ -610,6 +803,7 @@ def main():
     ap.add_argument("--nz", type=int, default=64, help="slices for --network-forward")
     ap.add_argument("--reps", type=int, default=5, help="forward passes timed by --network-forward")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other", action="store_true", help="skip the 4D workloads after the headline one")
     ap.add_argument("--no-converge", action="store_true", help="skip the seconds-to-converged-cost run")
     args = ap.parse_args()
     if args.network_forward:

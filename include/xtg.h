@@ -96,6 +96,9 @@ int xtg_get_hr(const xtg_ctx *ctx, float *hr /*[N_p][65]*/);
 /* Options: A storage, update order, concurrent columns (0 = device default),
  * seed of the GPU visiting order. */
 int xtg_set_options(xtg_ctx *ctx, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed);
+/* The options in force (XTG_A_AUTO resolved to the storage it picked);
+ * outputs may be NULL.  No reference counterpart. */
+int xtg_get_options(const xtg_ctx *ctx, int32_t *a_mode, int32_t *order, int32_t *max_columns, uint64_t *seed);
 /* Parallel schedule: z slices per ICD work piece (0 = chosen from the L2 size,
  * the default).  Each column visit is cut into pieces of at most this many
  * slices, visited piece-major, so the error-sinogram and weight rows in

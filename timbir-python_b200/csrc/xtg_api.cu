@@ -1431,6 +1431,14 @@ static int count_table(xtg_ctx *c, std::vector<long long> &cnt, long long *total
 
 // XTG_A_AUTO: the exact FP32 table when it fits in free device memory with
 // 2 GiB to spare, else the FP16 table, else entries computed per visit.
+int xtg_get_options(const xtg_ctx *c, int32_t *a_mode, int32_t *order, int32_t *max_columns, uint64_t *seed) {
+  if (!c) return XTG_E_ARG;
+  if (a_mode) *a_mode = c->a_mode;
+  if (order) *order = c->order;
+  if (max_columns) *max_columns = c->max_columns;
+  if (seed) *seed = c->seed;
+  return 0;
+}
 static int choose_amode(xtg_ctx *c, int *mode) {
   std::vector<long long> cnt;
   long long run = 0, mx = 0;
