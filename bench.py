@@ -224,6 +224,105 @@ def network_roofline(ctx, net, coarse_iters, reps=3):
             "frac": flops / ms / 1e9 / peak, "peak_kind": kind, "bound": "tensor"}
 
 
+def projector_timing(ctx, reps=3):
+    """Forward-projection calls on the resident (zero) object, each through
+    the C ABI (which synchronises its stream): e = y - Ax - d in FP32 (the
+    reference's order) and the FP64 resync, with the bin-major A table (the
+    default where it fits) and with the table-free gather.  Algorithmic HBM
+    bytes of one table launch: y read + e written (+ w read for the resync's
+    cost) + 8 B per table entry; the object (a z-line per entry) is re-read
+    from L2 and L1."""
+    import torch
+    out = {}
+    for kind, key in ((xtg.XTG_PROJ_GATHER, "gather"), (xtg.XTG_PROJ_AUTO, "table")):
+        ctx.set_projector(kind)
+        ctx.init_error_sino()  # builds the table (outside the timing)
+        r = {}
+        for name, fn in (("init_error_ms", ctx.init_error_sino), ("resync_fp64_ms", ctx.resync_fp64)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                fn()
+            r[name] = (time.perf_counter() - t0) * 1e3 / reps
+        used, entries = ctx.projector()
+        if key == "table":
+            out["kind"] = "table" if used == xtg.XTG_PROJ_TABLE else "gather"
+            if used == xtg.XTG_PROJ_TABLE:
+                ns = int(np.prod(ctx.sino_shape))
+                peak, _ = peaks()
+                alg = {"init_error_ms": 8.0 * ns + 8.0 * entries, "resync_fp64_ms": 12.0 * ns + 8.0 * entries}
+                r["table_entries"] = entries
+                r["hbm_gbs_alg"] = {k: alg[k] / (r[k] / 1e3) / 1e9 for k in alg}
+                r["frac_of_measured_hbm"] = {k: alg[k] / (r[k] / 1e3) / 1e9 / peak for k in alg}
+        out[key] = r
+    return out
+
+
+def kernel_timings(args, reps=5):
+    """`--kernels`: the engine's other north-star kernels, each through its C
+    ABI call on the workload (after the FBP start and two iterations, so the
+    object and the error sinogram are realistic), timed on the host around
+    the call (the call synchronises the library's stream; the mean of `reps`
+    calls), with the algorithmic HBM bytes of one call and their rate against
+    the measured copy bandwidth.  Bytes: sinogram arrays 4 B per entry each
+    (e, w, y read; e written), the bin-major A table 8 B per entry, the
+    object 4 B per voxel (its neighbours come from L1/L2), the NHICD maps
+    4 B per value per pass.  The ncu summaries in profiles/ capture the same
+    command."""
+    import torch
+    w = workload(args)
+    p, t, a, x_true, y, wt = make_data(w)
+    ctx = xtg.Context(p, t, a)
+    ctx.set_options(a_mode=xtg.XTG_A_TABLE32)
+    ctx.upload_sino(y, wt)
+    ctx.init_fbp()
+    for it in (1, 2):
+        ctx.iteration(it)
+    ns = int(np.prod(ctx.sino_shape))
+    nvox = int(np.prod(ctx.obj_shape))
+    _, entries = ctx.projector()
+    nmag = int(np.prod(ctx.mag_shape))
+    usn = np.full(ctx.N_time * ctx.nzb, ctx.n_masked, np.int32)
+    peak, kind = peaks()
+    calls = {
+        # name: (call, algorithmic bytes, kernels)
+        "init_error_sino": (ctx.init_error_sino, 8.0 * ns + 8.0 * entries, "k_fp_csr<1>"),
+        "resync_fp64": (ctx.resync_fp64, 12.0 * ns + 8.0 * entries + 4.0 * nvox, "k_fp_csr<2>, k_prior_cost64"),
+        "map_cost_fp64": (ctx.cost, 8.0 * ns + 8.0 * entries + 4.0 * nvox, "k_fp_csr<3>, k_prior_cost64"),
+        "map_cost_running": (ctx.cost_running, 8.0 * ns + 4.0 * nvox, "k_running_cost64, k_prior_cost64"),
+        "zinger_refresh": (lambda: ctx.zinger_refresh(want_mask=False), 8.0 * ns, "k_zinger_refresh"),
+        "nhicd_select": (lambda: ctx.nhicd_select(usn), 4.0 * nmag * 6, "k_vsc_filter, k_rs_hist, k_rs_pick, "
+                                                                         "k_nhicd_compact"),
+    }
+    out = {"workload": workload_name(w), "sinogram_entries": ns, "voxels": nvox, "table_entries": entries,
+           "peak_gbs": peak, "peak_kind": peak_kind_note(kind), "calls": {}}
+    for name, (fn, alg, kern) in calls.items():
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        ms = (time.perf_counter() - t0) * 1e3 / reps
+        gbs = alg / (ms / 1e3) / 1e9
+        out["calls"][name] = {"ms": ms, "alg_bytes": alg, "gbs": gbs, "frac": gbs / peak, "kernels": kern}
+    # the A column table of the ICD kernel: an iteration that rebuilds it
+    # against one that does not
+    its = []
+    for rebuild in (False, True):
+        if rebuild:
+            ctx.set_options(a_mode=xtg.XTG_A_FP16)
+            ctx.set_options(a_mode=xtg.XTG_A_TABLE32)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.iteration(3)
+        torch.cuda.synchronize()
+        its.append((time.perf_counter() - t0) * 1e3)
+    out["calls"]["column_table_build"] = {"ms": its[1] - its[0], "kernels": "k_table_count, k_table_fill",
+                                          "note": "iteration with the rebuild minus one without"}
+    ctx.close()
+    print(json.dumps(out), flush=True)
+
+
 def network_forward(nxy, nz, reps, weights=WEIGHTS):
     """`--network-forward`: the warm-start network's forward pass alone (the
     inference inside the learned start) on one volume [1][nxy][nxy][nz] of
@@ -409,10 +508,8 @@ def run_ours(args):
     ctx.set_zslab(args.zslab)
     ctx.upload_sino(y, wt)
     ctx.init_error_sino()
-    torch.cuda.synchronize()
-    tf = time.perf_counter()
-    ctx.init_error_sino()  # e = y - Ax - d (fast projector), timed once for the log
-    fp_ms = (time.perf_counter() - tf) * 1e3
+    proj = projector_timing(ctx) if world == 1 else None
+    fp_ms = proj["table" if proj["kind"] == "table" else "gather"]["init_error_ms"] if proj else None
     nnz = nnz_per_column(ctx, p, t, a)
     it = 0
     for _ in range(args.warmup):
@@ -482,7 +579,7 @@ def run_ours(args):
                    "iterations_timed": [args.warmup + 1, args.warmup + args.steps],
                    "l2": f"inputs larger than L2 (e + w = {2 * y.nbytes / 1e6:.0f} MB)",
                    "parallelism": f"replicas{world}",
-                   "cost_after": cost, "wall_s_timed": wall, "forward_projection_ms": fp_ms,
+                   "cost_after": cost, "wall_s_timed": wall, "forward_projection_ms": fp_ms, "projector": proj,
                    "zero_skipped_per_step": zsk / args.steps,
                    "counted": "voxel updates exclude zero-skipped voxels (x = 0 with no positive neighbour)"},
         "e2e": {"value": e2e, "unit": "voxel-updates/s", "h2d_bytes_per_step": int(y.nbytes + wt.nbytes),
@@ -802,12 +899,16 @@ def main():
                     help="time only the warm-start network's forward pass on [1][nxy][nxy][nz] (profiling)")
     ap.add_argument("--nz", type=int, default=64, help="slices for --network-forward")
     ap.add_argument("--reps", type=int, default=5, help="forward passes timed by --network-forward")
+    ap.add_argument("--kernels", action="store_true",
+                    help="time the non-ICD kernels of the engine on the workload (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-other", action="store_true", help="skip the 4D workloads after the headline one")
     ap.add_argument("--no-converge", action="store_true", help="skip the seconds-to-converged-cost run")
     args = ap.parse_args()
     if args.network_forward:
         network_forward(args.nxy or 512, args.nz, args.reps)
+    elif args.kernels:
+        kernel_timings(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

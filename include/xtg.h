@@ -96,6 +96,21 @@ int xtg_get_hr(const xtg_ctx *ctx, float *hr /*[N_p][65]*/);
 /* Options: A storage, update order, concurrent columns (0 = device default),
  * seed of the GPU visiting order. */
 int xtg_set_options(xtg_ctx *ctx, int32_t a_mode, int32_t order, int32_t max_columns, uint64_t seed);
+/* Forward projector.  Both give the same values (bit-identical in FP32, the
+ * reference's summation order; FP64 sums otherwise):
+ *   XTG_PROJ_AUTO:   at the first projection the context builds a bin-major
+ *                    A table (rows (view, bin), entries in the reference's
+ *                    (row, column) order; 8 B per entry) when it fits in free
+ *                    device memory next to the ICD column table and 2 GiB to
+ *                    spare, and projects from it; else as XTG_PROJ_GATHER.
+ *   XTG_PROJ_GATHER: A evaluated on the fly for each (view, 32 bins), no
+ *                    table.
+ * xtg_get_projector reports XTG_PROJ_TABLE once the table is in use (or
+ * XTG_PROJ_GATHER; XTG_PROJ_AUTO before the first projection) and its entry
+ * count.  No reference counterpart (B200 layout choices). */
+enum { XTG_PROJ_AUTO = 0, XTG_PROJ_GATHER = 1, XTG_PROJ_TABLE = 2 };
+int xtg_set_projector(xtg_ctx *ctx, int32_t kind);
+int xtg_get_projector(const xtg_ctx *ctx, int32_t *in_use, int64_t *table_entries);
 /* The options in force (XTG_A_AUTO resolved to the storage it picked);
  * outputs may be NULL.  No reference counterpart. */
 int xtg_get_options(const xtg_ctx *ctx, int32_t *a_mode, int32_t *order, int32_t *max_columns, uint64_t *seed);

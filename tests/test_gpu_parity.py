@@ -71,11 +71,40 @@ def test_amatrix_exhaustive_plain3d():
         assert cnt[q] == len(ov) and np.array_equal(vals[q, :cnt[q]], ov) and np.array_equal(idx[q, :cnt[q]], oi)
 
 
+@pytest.mark.parametrize("kind", [xtg.XTG_PROJ_AUTO, xtg.XTG_PROJ_GATHER])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_forward_projection_bit_exact(name):
+def test_forward_projection_bit_exact(name, kind):
     c, g, _ = ctx_for(name)
+    c.set_projector(kind)
     c.upload_object(g["x_true"])
     assert np.array_equal(c.forward_project(), g["ax"])
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_projectors_agree(name):
+    """The bin-major-table projector (the default where it fits) and the
+    table-free gather give identical results: A x and e = y - Ax - d bit for
+    bit (both sum in the reference's order), the FP64 resync's e and cost
+    too (FP64 sums in the same order; products of FP32 values are exact)."""
+    c, g, _ = ctx_for(name)
+    c.upload_sino(g["y"], g["w"])
+    c.upload_object(g["x_true"] * 0.7)
+    out = {}
+    for kind in (xtg.XTG_PROJ_AUTO, xtg.XTG_PROJ_GATHER):
+        c.set_projector(kind)
+        ax = c.forward_project()
+        c.init_error_sino()
+        e1 = c.error_sino()
+        cost = c.cost()
+        rs = c.resync_fp64()
+        out[kind] = (ax, e1, cost, rs, c.error_sino(), c.projector())
+    a, b = out[xtg.XTG_PROJ_AUTO], out[xtg.XTG_PROJ_GATHER]
+    assert a[5][0] == xtg.XTG_PROJ_TABLE and a[5][1] > 0
+    assert b[5] == (xtg.XTG_PROJ_GATHER, 0)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert np.array_equal(a[4], b[4])
+    for x, y in zip(a[2] + a[3], b[2] + b[3]):
+        assert x == pytest.approx(y, rel=1e-13, abs=1e-12)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

@@ -87,6 +87,13 @@ struct xtg_ctx {
   float *d_tval32 = nullptr, *d_tscale = nullptr;
   __half *d_tval16 = nullptr;
   int table_mode = 0;  // 0 none, XTG_A_FP16 or XTG_A_TABLE32 when built
+  // bin-major A table of the projector (rows (view, bin)); csr_state 0 = not
+  // tried yet, 1 = built, -1 = not used (does not fit, or the gather projector
+  // was requested)
+  long long *d_cptr = nullptr;
+  int2 *d_cent = nullptr;
+  int csr_state = 0, projector = XTG_PROJ_AUTO;
+  long long csr_nnz = 0;
   long long table_nnz = 0;
   int table_max = 0;
   // options
@@ -588,13 +595,80 @@ static DevGeo make_devgeo(const xt_geom &g, int positivity) {
   return G;
 }
 
+static double fp_win_margin(const xtg_ctx *c) { return 1e-4 * (double)c->g.N_r * c->g.delta_r + 1e-3 * c->g.delta_r; }
+
+// The projector's bin-major A table, built at the first projection of the
+// context when it fits in free device memory next to the column table the
+// ICD kernel may still build (and 2 GiB to spare); otherwise the projector
+// evaluates A on the fly (k_fp_bins).  Only CUDA errors are returned.
+static cudaError_t ensure_csr(xtg_ctx *c) {
+  if (c->csr_state) return cudaSuccess;
+  c->csr_state = -1;
+  if (c->projector == XTG_PROJ_GATHER) return cudaSuccess;
+  // entries hold a z-line's element offset within its frame as an int32
+  if ((size_t)c->g.N_y * c->g.N_x * c->g.N_z >= ((size_t)1 << 31)) return cudaSuccess;
+  const size_t rows = (size_t)c->g.N_p * c->g.N_r;
+  int *d_cnt = nullptr;
+  if (cudaMalloc(&d_cnt, rows * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
+  CsrBuildArgs B;
+  memset(&B, 0, sizeof(B));
+  B.hr = c->d_hr; B.cosv = c->d_cos; B.sinv = c->d_sin; B.win_margin = fp_win_margin(c); B.count = d_cnt;
+  cudaError_t e = launch_csr_build(c->G, B, 0, c->span, c->st);
+  std::vector<int> cnt(rows);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt.data(), d_cnt, rows * 4, cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  cudaFree(d_cnt);
+  c->launches++;
+  if (e != cudaSuccess) return e;
+  std::vector<long long> ptr(rows + 1, 0);
+  for (size_t i = 0; i < rows; i++) ptr[i + 1] = ptr[i] + cnt[i];
+  const long long nnz = ptr[rows];
+  size_t fr = 0, tot = 0;
+  if ((e = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return e;
+  // the column table, if one is still to be built, has at most as many entries
+  const size_t pending = (c->a_mode != XTG_A_FP32 && c->table_mode == 0) ? (size_t)nnz * 8 : 0;
+  const size_t need = (size_t)nnz * 8 + (rows + 1) * 8;
+  if (need + pending + ((size_t)2 << 30) > fr) return cudaSuccess;
+  if (cudaMalloc(&c->d_cptr, (rows + 1) * 8) != cudaSuccess || cudaMalloc(&c->d_cent, (size_t)nnz * 8 + 8) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(c->d_cptr);
+    cudaFree(c->d_cent);
+    c->d_cptr = nullptr;
+    c->d_cent = nullptr;
+    return cudaSuccess;
+  }
+  c->dev_bytes += need + 8;
+  if ((e = cudaMemcpyAsync(c->d_cptr, ptr.data(), (rows + 1) * 8, cudaMemcpyHostToDevice, c->st)) != cudaSuccess)
+    return e;
+  B.count = nullptr;
+  B.ptr = c->d_cptr;
+  B.ent = c->d_cent;
+  if ((e = launch_csr_build(c->G, B, 1, c->span, c->st)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(c->st)) != cudaSuccess) return e;
+  c->launches++;
+  c->csr_nnz = nnz;
+  c->csr_state = 1;
+  return cudaSuccess;
+}
+
 template <int MODE>
 static cudaError_t launch_fp(xtg_ctx *c, float *out, double *slots) {
+  cudaError_t e = ensure_csr(c);
+  if (e != cudaSuccess) return e;
   FpArgs F;
   F.x = c->d_x; F.y = c->d_y; F.d = c->d_d; F.w = c->d_w; F.hr = c->d_hr; F.cosv = c->d_cos; F.sinv = c->d_sin;
   F.fov = c->d_fov; F.out = out; F.cost_slots = slots; F.T = c->g.T; F.delta = c->g.delta;
-  F.win_margin = 1e-4 * (double)c->g.N_r * c->g.delta_r + 1e-3 * c->g.delta_r;
+  F.win_margin = fp_win_margin(c);
   c->launches++;
+  if (c->csr_state == 1) {
+    CsrView T;
+    T.ptr = c->d_cptr;
+    T.ent = c->d_cent;
+    return xtg::launch_fp_csr(c->G, F, T, MODE, c->st);
+  }
   return xtg::launch_fp(c->G, F, MODE, c->span, c->st);
 }
 
@@ -610,7 +684,7 @@ void xtg_destroy(xtg_ctx *c) {
                   c->d_filt, c->d_tmp, c->d_num, c->d_den, c->d_thr, c->d_var, c->d_view_idx, c->d_view_start,
                   c->d_view_num, c->d_fov, c->d_mcols, c->d_rank, c->d_counter, c->d_nhcnt, c->d_err, c->d_kth,
                   c->d_items, c->d_nh, c->d_red, c->d_absx, c->d_cnt, c->d_tstart, c->d_toff, c->d_tval32,
-                  c->d_tscale, c->d_tval16, c->d_rs_hist, c->d_rs_st};
+                  c->d_tscale, c->d_tval16, c->d_rs_hist, c->d_rs_st, c->d_cptr, c->d_cent};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1431,6 +1505,29 @@ static int count_table(xtg_ctx *c, std::vector<long long> &cnt, long long *total
 
 // XTG_A_AUTO: the exact FP32 table when it fits in free device memory with
 // 2 GiB to spare, else the FP16 table, else entries computed per visit.
+int xtg_set_projector(xtg_ctx *c, int32_t kind) {
+  if (!c || (kind != XTG_PROJ_AUTO && kind != XTG_PROJ_GATHER)) {
+    set_err("xtg_set_projector: bad projector kind");
+    return XTG_E_ARG;
+  }
+  if (kind != c->projector) {
+    cudaFree(c->d_cptr);
+    cudaFree(c->d_cent);
+    if (c->csr_state == 1) c->dev_bytes -= (size_t)c->csr_nnz * 8 + ((size_t)c->g.N_p * c->g.N_r + 2) * 8;
+    c->d_cptr = nullptr;
+    c->d_cent = nullptr;
+    c->csr_state = 0;
+    c->csr_nnz = 0;
+    c->projector = kind;
+  }
+  return 0;
+}
+int xtg_get_projector(const xtg_ctx *c, int32_t *in_use, int64_t *table_entries) {
+  if (!c) return XTG_E_ARG;
+  if (in_use) *in_use = c->csr_state == 1 ? XTG_PROJ_TABLE : c->csr_state == -1 ? XTG_PROJ_GATHER : XTG_PROJ_AUTO;
+  if (table_entries) *table_entries = c->csr_nnz;
+  return 0;
+}
 int xtg_get_options(const xtg_ctx *c, int32_t *a_mode, int32_t *order, int32_t *max_columns, uint64_t *seed) {
   if (!c) return XTG_E_ARG;
   if (a_mode) *a_mode = c->a_mode;

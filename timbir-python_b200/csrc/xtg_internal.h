@@ -50,6 +50,19 @@ struct FpArgs {
   double win_margin;
 };
 
+// bin-major A table: row (view p, bin r) = entries [ptr[p N_r + r], ptr[p N_r + r + 1])
+struct CsrBuildArgs {
+  const float *hr, *cosv, *sinv;
+  double win_margin;
+  int *count;           // build pass 0: entries per row
+  const long long *ptr; // build pass 1: row starts
+  int2 *ent;            // {(j * N_x + k) * N_z, bits of its A (without delta_t)} per entry
+};
+struct CsrView {
+  const long long *ptr;
+  const int2 *ent;
+};
+
 struct TableArgs {
   const float *hr, *cosv, *sinv;
   const int *view_idx, *view_start, *view_num, *mcols;
@@ -62,6 +75,8 @@ struct TableArgs {
 };
 
 cudaError_t launch_fp(const DevGeo &G, const FpArgs &F, int mode, int ns, cudaStream_t st);
+cudaError_t launch_csr_build(const DevGeo &G, const CsrBuildArgs &B, int fill, int ns, cudaStream_t st);
+cudaError_t launch_fp_csr(const DevGeo &G, const FpArgs &F, const CsrView &T, int mode, cudaStream_t st);
 cudaError_t launch_table_count(const DevGeo &G, const TableArgs &T, int ns, long long *count, cudaStream_t st);
 cudaError_t launch_table_fill(const DevGeo &G, const TableArgs &T, int ns, cudaStream_t st);
 

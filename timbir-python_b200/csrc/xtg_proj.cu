@@ -203,6 +203,227 @@ cudaError_t launch_fp(const DevGeo &G, const FpArgs &F, int mode, int ns, cudaSt
   }
 }
 
+// ------------------------------------------------ bin-major A table ------
+// The A entries regrouped by sinogram row (view p, detector bin r): row
+// (p, r) lists (column j N_x + k, A) for every column of p's frame that
+// reaches bin r, in increasing (j, k) -- the order in which the reference
+// adds a column's contribution to that entry (initErrorSinogam,
+// XT_ICD_update.c:551-569).  Built once per context by the enumeration of
+// k_fp_bins, so every value is the exact A of calcAMatrixColumnforAngle
+// (XT_AMatrix.c:50-110).  Lane b of a warp owns bin rb + b of the warp's 32
+// bins: for each hit column the lanes test their own bin in parallel, so the
+// appends of a bin stay in column order without atomics.
+template <int FILL, int NS>
+__global__ void __launch_bounds__(FP_WARPS * 32) k_csr_build(DevGeo G, CsrBuildArgs B) {
+  extern __shared__ __align__(16) unsigned char cb_sm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float *vsm = reinterpret_cast<float *>(cb_sm) + (size_t)warp * 32 * NS;
+  const int p = blockIdx.x;
+  const int rb = (blockIdx.y * FP_WARPS + warp) * 32;
+  if (rb >= G.N_r) return;  // whole warp; no block-wide barrier follows
+  const float cp = B.cosv[p], sp = B.sinv[p];
+  const float *H = B.hr + (size_t)p * XT_HR_STRIDE;
+  const double lo = (double)G.R0 + (double)rb * G.delta_r - G.delta_xy - B.win_margin;
+  const double hi = (double)G.R0 + (double)(rb + 32) * G.delta_r + G.delta_xy + B.win_margin;
+  const int r = rb + lane;
+  const bool own = r < G.N_r;
+  long long cur = 0;
+  int cnt = 0;
+  if (FILL && own) cur = B.ptr[(size_t)p * G.N_r + r];
+  for (int j = 0; j < G.N_y; j++) {
+    int klo, khi;
+    if (!fp_col_range(G, cp, sp, xt_coord(G.y0, j, G.delta_xy), lo, hi, &klo, &khi)) continue;
+    for (int kb = klo; kb <= khi; kb += 32) {
+      const int k = kb + lane;
+      float v[NS];
+#pragma unroll
+      for (int q = 0; q < NS; q++) v[q] = 0.f;
+      int first = 0, n = 0;
+      if (k <= khi) n = xt_amatrix_regs<NS>(G, H, cp, sp, j, k, v, &first);
+      const int slo = max(0, rb - first), shi = min(n, rb + 32 - first);
+      const unsigned hit = __ballot_sync(0xffffffffu, slo < shi);
+      if (!hit) continue;
+#pragma unroll
+      for (int q = 0; q < NS; q++) vsm[lane * NS + q] = v[q];
+      const int pk = (int)(((unsigned)(first - rb + 64) << 16) | ((unsigned)slo << 8) | (unsigned)shi);
+      __syncwarp();
+      unsigned mk = hit;
+      while (mk) {
+        const int l = __ffs(mk) - 1;
+        mk &= mk - 1;
+        const int q = __shfl_sync(0xffffffffu, pk, l);
+        const int sl = (q >> 8) & 0xFF, sh = q & 0xFF;
+        const int sidx = lane - ((q >> 16) - 64);  // this lane's bin within the column's run
+        if (own && sidx >= sl && sidx < sh) {
+          const float a = vsm[l * NS + sidx];
+          if (a != 0.f) {
+            if (FILL) {
+              B.ent[cur] = make_int2((j * G.N_x + kb + l) * G.N_z, __float_as_int(a));
+              cur++;
+            } else {
+              cnt++;
+            }
+          }
+        }
+      }
+      __syncwarp();  // the staged entries are rewritten by the next round
+    }
+  }
+  if (!FILL && own) B.count[(size_t)p * G.N_r + r] = cnt;
+}
+
+template <int FILL>
+static cudaError_t launch_csr_build_t(const DevGeo &G, const CsrBuildArgs &B, int ns, cudaStream_t st) {
+  const int nsv = ns <= 3 ? 3 : ns <= 4 ? 4 : 12;
+  const size_t smem = (size_t)FP_WARPS * 32 * nsv * sizeof(float);
+  dim3 grid((unsigned)G.N_p, (unsigned)((G.N_r + FP_WARPS * 32 - 1) / (FP_WARPS * 32)));
+  if (ns <= 3)
+    k_csr_build<FILL, 3><<<grid, FP_WARPS * 32, smem, st>>>(G, B);
+  else if (ns <= 4)
+    k_csr_build<FILL, 4><<<grid, FP_WARPS * 32, smem, st>>>(G, B);
+  else
+    k_csr_build<FILL, 12><<<grid, FP_WARPS * 32, smem, st>>>(G, B);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_csr_build(const DevGeo &G, const CsrBuildArgs &B, int fill, int ns, cudaStream_t st) {
+  return fill ? launch_csr_build_t<1>(G, B, ns, st) : launch_csr_build_t<0>(G, B, ns, st);
+}
+
+// Forward projection from the bin-major table: one warp per sinogram row
+// (view, bin) and 64 detector rows.  Every lane reads each entry
+// {z-line offset, A} (a broadcast from L1; two entries per 16-byte load) and
+// its rows of that z-line (PAIR: rows 2 lane, 2 lane + 1 as one 8-byte load
+// when a slice covers one detector row; the warp's loads form one 256-byte
+// run), and accumulates in registers, entries in table order: in FP32
+// (__fadd_rn(__fmul_rn)) that is the reference's summation order, so MODE
+// 0 / 1 are bit-identical to k_fp_bins and to initErrorSinogam; MODE 2 / 3
+// accumulate in FP64 in the same order (a product of two FP32 values is
+// exact in FP64, so the sums equal k_fp_bins' bit for bit).  Eight entries
+// are loaded before any is added.  The eight warps of a CTA take eight
+// consecutive bins of one view, which share most of their columns, so many
+// z-lines are L1 hits.  FULL: every 64-row chunk is complete (N_t a multiple
+// of 64), so no lane needs a bounds test.
+#define CSR_WARPS 8
+template <int MODE, typename ACC, bool PAIR, bool FULL>
+__global__ void __launch_bounds__(CSR_WARPS * 32) k_fp_csr(DevGeo G, FpArgs F, CsrView T) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int p = blockIdx.x;
+  const int r = blockIdx.y * CSR_WARPS + warp;
+  if (r >= G.N_r) return;  // whole warp; no block-wide barrier follows
+  const int t0 = blockIdx.z * 64, nt = FULL ? 64 : min(64, G.N_t - t0);
+  // rows of this lane: PAIR (zovl == 1, N_t even): 2 lane, 2 lane + 1, one
+  // float2 at slice t0 + 2 lane; otherwise lane and lane + 32
+  const int ta = PAIR ? 2 * lane : lane, tb = PAIR ? 2 * lane + 1 : lane + 32;
+  const bool va = FULL || ta < nt, vb = FULL || tb < nt;
+  const float *xf = F.x + (size_t)F.fov[p] * G.N_y * G.N_x * G.N_z;
+  const float *xla = xf + (t0 + ta) / G.zovl, *xlb = xf + (t0 + tb) / G.zovl;
+  const long long e0 = T.ptr[(size_t)p * G.N_r + r], e1 = T.ptr[(size_t)p * G.N_r + r + 1];
+  ACC acc_a = (ACC)0, acc_b = (ACC)0;
+  auto add = [&](float xa, float xb, float a) {
+    if (MODE <= 1) {
+      acc_a = __fadd_rn(acc_a, __fmul_rn(xa, a));
+      acc_b = __fadd_rn(acc_b, __fmul_rn(xb, a));
+    } else {
+      acc_a += (ACC)xa * (ACC)a;
+      acc_b += (ACC)xb * (ACC)a;
+    }
+  };
+  auto load = [&](int off, float &xa, float &xb) {
+    if (PAIR) {
+      const float2 v = va ? __ldg(reinterpret_cast<const float2 *>(xla + off)) : make_float2(0.f, 0.f);
+      xa = v.x;
+      xb = v.y;
+    } else {
+      xa = va ? __ldg(xla + off) : 0.f;
+      xb = vb ? __ldg(xlb + off) : 0.f;
+    }
+  };
+  long long i = e0;
+  if (i < e1 && (i & 1)) {  // to a 16-byte boundary of the entry array
+    const int2 en = __ldg(T.ent + i);
+    float xa, xb;
+    load(en.x, xa, xb);
+    add(xa, xb, __int_as_float(en.y));
+    i++;
+  }
+  for (; i + 8 <= e1; i += 8) {
+    const int4 *q = reinterpret_cast<const int4 *>(T.ent + i);
+    int4 qv[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) qv[u] = __ldg(q + u);
+    float xa[8], xb[8];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      load(qv[u].x, xa[2 * u], xb[2 * u]);
+      load(qv[u].z, xa[2 * u + 1], xb[2 * u + 1]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      add(xa[2 * u], xb[2 * u], __int_as_float(qv[u].y));
+      add(xa[2 * u + 1], xb[2 * u + 1], __int_as_float(qv[u].w));
+    }
+  }
+  for (; i < e1; i++) {
+    const int2 en = __ldg(T.ent + i);
+    float xa, xb;
+    load(en.x, xa, xb);
+    add(xa, xb, __int_as_float(en.y));
+  }
+  double cacc = 0.0;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int t = h ? tb : ta;
+    if (!FULL && t >= nt) continue;
+    const ACC sacc = h ? acc_b : acc_a;
+    const size_t o = ((size_t)p * G.N_r + r) * G.N_t + t0 + t;
+    const size_t od = (size_t)r * G.N_t + t0 + t;
+    if (MODE == 0) {
+      F.out[o] = (float)sacc;
+    } else if (MODE == 1) {
+      F.out[o] = __fsub_rn(__fsub_rn(F.y[o], (float)sacc), F.d[od]);
+    } else {
+      // A * delta_t: the system matrix of the voxel update (XT_VoxUpdate.c:27, 67)
+      const double e64 = (double)F.y[o] - (double)G.delta_t * (double)sacc - (double)F.d[od];
+      if (MODE == 2) F.out[o] = (float)e64;
+      const double sw = e64 * sqrt((double)F.w[o]);
+      if (fabs(sw) < (double)F.T)
+        cacc += sw * sw;
+      else
+        cacc += 2.0 * (double)F.delta * (double)F.T * fabs(sw) + (double)F.T * (double)F.T * (1.0 - 2.0 * (double)F.delta);
+    }
+  }
+  if (MODE >= 2) {
+    for (int off = 16; off > 0; off >>= 1) cacc += __shfl_xor_sync(0xffffffffu, cacc, off);
+    if (lane == 0) atomicAdd(&F.cost_slots[(blockIdx.x * 7 + r + blockIdx.z) % 64], cacc);
+  }
+}
+
+template <bool PAIR, bool FULL>
+static void launch_fp_csr_t(const DevGeo &G, const FpArgs &F, const CsrView &T, int mode, cudaStream_t st) {
+  dim3 grid((unsigned)G.N_p, (unsigned)((G.N_r + CSR_WARPS - 1) / CSR_WARPS), (unsigned)((G.N_t + 63) / 64));
+  switch (mode) {
+    case 0: k_fp_csr<0, float, PAIR, FULL><<<grid, CSR_WARPS * 32, 0, st>>>(G, F, T); break;
+    case 1: k_fp_csr<1, float, PAIR, FULL><<<grid, CSR_WARPS * 32, 0, st>>>(G, F, T); break;
+    case 2: k_fp_csr<2, double, PAIR, FULL><<<grid, CSR_WARPS * 32, 0, st>>>(G, F, T); break;
+    default: k_fp_csr<3, double, PAIR, FULL><<<grid, CSR_WARPS * 32, 0, st>>>(G, F, T); break;
+  }
+}
+
+cudaError_t launch_fp_csr(const DevGeo &G, const FpArgs &F, const CsrView &T, int mode, cudaStream_t st) {
+  // paired rows need one detector row per slice, an even row count (so a
+  // chunk never ends inside a pair) and 8-byte aligned z-lines
+  if (G.zovl == 1 && G.N_t % 2 == 0 && G.N_z % 2 == 0) {
+    if (G.N_t % 64 == 0)
+      launch_fp_csr_t<true, true>(G, F, T, mode, st);
+    else
+      launch_fp_csr_t<true, false>(G, F, T, mode, st);
+  } else {
+    launch_fp_csr_t<false, false>(G, F, T, mode, st);
+  }
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------- A column table --
 // entries of (frame f, masked column ci): one warp, lanes over views
 template <int NS>

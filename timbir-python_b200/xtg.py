@@ -23,12 +23,13 @@ LIBDIR = os.path.join(HERE, "lib")
 XTG_A_FP32, XTG_A_FP16, XTG_A_TABLE32, XTG_A_AUTO = 0, 1, 2, 3
 XTG_ORDER_PARALLEL, XTG_ORDER_SEQUENTIAL = 0, 1
 XTG_MULTIRES_Z, XTG_MULTIRES_BIN = 1, 2
+XTG_PROJ_AUTO, XTG_PROJ_GATHER, XTG_PROJ_TABLE = 0, 1, 2
 
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
     "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_init_object_fbp", "xtg_object_to_device",
     "xtg_object_from_device", "xtg_upsample", "xtg_init_object_multires", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
-    "xtg_get_hr", "xtg_set_options", "xtg_get_options", "xtg_upload_sino", "xtg_upload_sino_start", "xtg_upload_counts", "xtg_upload_object",
+    "xtg_get_hr", "xtg_set_options", "xtg_get_options", "xtg_set_projector", "xtg_get_projector", "xtg_upload_sino", "xtg_upload_sino_start", "xtg_upload_counts", "xtg_upload_object",
     "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
     "xtg_get_offset", "xtg_set_offset", "xtg_get_magmap", "xtg_set_magmap", "xtg_get_variance",
     "xtg_set_variance", "xtg_amatrix", "xtg_forward_project", "xtg_init_error_sino",
@@ -331,6 +332,15 @@ class Context:
 
     def set_options(self, a_mode=XTG_A_FP32, order=XTG_ORDER_PARALLEL, max_columns=0, seed=0x5EED5EED):
         _check(self.lib.xtg_set_options(self.h, a_mode, order, max_columns, seed), "xtg_set_options")
+
+    def set_projector(self, kind):
+        _check(self.lib.xtg_set_projector(self.h, int(kind)), "xtg_set_projector")
+
+    def projector(self):
+        """(projector in use, entries of its bin-major table)."""
+        k, n = C.c_int32(), C.c_int64()
+        _check(self.lib.xtg_get_projector(self.h, C.byref(k), C.byref(n)), "xtg_get_projector")
+        return k.value, n.value
 
     def a_mode_used(self):
         """The A storage in force (XTG_A_AUTO resolved)."""
