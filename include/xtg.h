@@ -123,6 +123,32 @@ int xtg_set_zslab(xtg_ctx *ctx, int32_t slices);
 /* The z slices per work piece the parallel schedule uses now. */
 int xtg_get_zslab(const xtg_ctx *ctx, int32_t *slices);
 
+/* One z slab of a volume split over processes, one GPU each -- the
+ * reference's MPI ranks (XT_Init.c:290-294: a rank owns N_z / ranks slices
+ * and the matching N_t / ranks detector rows, Length_T / ranks).  Create the
+ * context with those N_t and length_t, then give it device planes
+ * [N_time][N_y][N_x] (caller-owned) for each side that has a neighbour:
+ * send_* receive this slab's boundary slice (slice 0 below, slice N_z - 1
+ * above), recv_* hold the neighbour's adjacent slice.  At the start of every
+ * xtg_icd_iteration and after each of its ICD launches (the reference
+ * exchanges after every half-pass, XT_ICD_update.c:816-880) the library
+ * fills send_*, drains its stream and calls exchange(user, phase); the hook
+ * moves the planes between processes (NCCL, MPI, ...) and returns 0 once
+ * recv_* hold the neighbours' slices.  The ICD updates then see those slices
+ * as z neighbours (XT_VoxUpdate.c:94-99), and the MAP cost's prior includes
+ * the pairs into the slab above (XT_ICD_update.c:203-205); summing the
+ * slabs' xtg_map_cost_fp64 and xtg_stats over processes gives the whole
+ * volume's cost and stop statistic.  NULL planes: no neighbour on that side.
+ * Variance and offset re-estimation are refused for slabs (they need sums
+ * over every slab inside the iteration). */
+typedef int (*xtg_exchange_fn)(void *user, int32_t phase);
+int xtg_set_slab(xtg_ctx *ctx, float *send_below, float *send_above, const float *recv_below, const float *recv_above,
+                 xtg_exchange_fn exchange, void *user);
+/* One exchange now (after the object changed outside xtg_icd_iteration, e.g.
+ * a warm start or an upload, and before a MAP cost); every slab of the volume
+ * must make the call. */
+int xtg_slab_exchange(xtg_ctx *ctx);
+
 /* genSinogram_fromBin + computeWriteSinogram (XT_genSinogram.c:264-300,
  * XT_Engine.c:89-121): y, w and the offset d (NULL = zero).  Weights are
  * divided by the variance estimate on the device, like the reference. */

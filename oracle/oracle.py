@@ -256,6 +256,24 @@ class Oracle(_Base):
         c = fn(C.c_void_p(self.h), C.byref(f), C.byref(p))
         return float(c), float(f.value), float(p.value)
 
+    def set_slab(self, below, above):
+        """This oracle is one z slab of a volume split over ranks."""
+        self.lib.xo_set_slab.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+        self.lib.xo_set_slab(C.c_void_p(self.h), int(below), int(above))
+
+    def boundary(self):
+        """(bottom slice, top slice), each [N_time][N_y][N_x]."""
+        lo, hi = self._arr((self.N_time, self.N_y, self.N_x)), self._arr((self.N_time, self.N_y, self.N_x))
+        self.lib.xo_get_boundary.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.xo_get_boundary(C.c_void_p(self.h), _ptr(lo), _ptr(hi))
+        return lo, hi
+
+    def set_halo(self, lo, hi):
+        lo = None if lo is None else np.ascontiguousarray(lo, self.real)
+        hi = None if hi is None else np.ascontiguousarray(hi, self.real)
+        self.lib.xo_set_halo.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.xo_set_halo(C.c_void_p(self.h), _ptr(lo), _ptr(hi))
+
     def init_error_sino_model(self):
         """e = y - delta_t A x - d (the voxel update's matrix)."""
         self.lib.xo_init_error_sino_model.argtypes = None

@@ -40,6 +40,9 @@ struct xo_ctx {
   uint8_t *mask;     /* [N_time][N_y][N_x][N_z] */
   xo_real *magmap;   /* [N_time][nzb][N_y][N_x] */
   int32_t *xr, *yr, *xn, *yn, *usn, *nsn;
+  /* z slab of a volume split over ranks: a neighbour below / above, whose
+   * adjacent slice sits in halo slice 0 / N_z + 1 (XT_Init.c:290-294) */
+  int32_t slab_lo, slab_hi;
 };
 
 #define OBJ(c, i, z, j, k) ((c)->obj[((((size_t)(i) * ((c)->N_z + 2) + (z)) * (c)->N_y + (j)) * (c)->N_x + (k))])
@@ -524,7 +527,8 @@ xo_real xo_cost(xo_ctx *c, xo_real *fwd_out, xo_real *prior_out) {
       }
   cost /= 2.0;
   temp = 0;
-  int Nz = c->N_z + 1;
+  /* ranks other than the last include the pairs into the halo above, XT_ICD_update.c:203-205 */
+  int Nz = c->slab_hi ? c->N_z + 2 : c->N_z + 1;
   const xo_real sq = c->Sigma_S_Q, sqp = c->Sigma_S_Q_P;
 #define XO_SV(d) xo_qggmrf_value(c, (d), sq, sqp, c->C_S)
   for (int i = 0; i < c->N_time; i++)
@@ -625,7 +629,7 @@ double xo_map_cost_fp64(const xo_ctx *c, double *fwd_out, double *prior_out) {
                 /* the 13 forward pairs: +x in the row, the next row, the next slice */
                 if (dz == 0 && (dy < 0 || (dy == 0 && dx <= 0))) continue;
                 const int jj = j + dy, kk = k + dx, zz = p + dz;
-                if (jj < 0 || jj >= c->N_y || kk < 0 || kk >= c->N_x || zz > c->N_z) continue;
+                if (jj < 0 || jj >= c->N_y || kk < 0 || kk >= c->N_x || zz > c->N_z + (c->slab_hi ? 1 : 0)) continue;
                 const double a = fabs(v - (double)OBJ(c, i, zz, jj, kk));
                 prior += (double)c->SF[1 + dz][1 + dy][1 + dx] * ((a * a / sq) / (cs + pow(a, 2.0 - mp) / sqp));
               }
@@ -638,6 +642,31 @@ double xo_map_cost_fp64(const xo_ctx *c, double *fwd_out, double *prior_out) {
   if (fwd_out) *fwd_out = fwd;
   if (prior_out) *prior_out = prior;
   return fwd + prior;
+}
+
+/* ------------------------------------------------------------ slabs ----- */
+void xo_set_slab(xo_ctx *c, int32_t below, int32_t above) {
+  c->slab_lo = below;
+  c->slab_hi = above;
+}
+
+/* this slab's boundary slices (1 and N_z of the haloed array), each
+ * [N_time][N_y][N_x] -- what MPI_Send_Recv_Z_Slices sends, XT_MPI.c:47-81 */
+void xo_get_boundary(const xo_ctx *c, xo_real *lo, xo_real *hi) {
+  const size_t pl = (size_t)c->N_y * c->N_x;
+  for (int i = 0; i < c->N_time; i++) {
+    if (lo) memcpy(lo + i * pl, &OBJ(c, i, 1, 0, 0), pl * sizeof(xo_real));
+    if (hi) memcpy(hi + i * pl, &OBJ(c, i, c->N_z, 0, 0), pl * sizeof(xo_real));
+  }
+}
+
+/* the neighbours' slices into halo slices 0 and N_z + 1 (NULL: unchanged) */
+void xo_set_halo(xo_ctx *c, const xo_real *lo, const xo_real *hi) {
+  const size_t pl = (size_t)c->N_y * c->N_x;
+  for (int i = 0; i < c->N_time; i++) {
+    if (lo) memcpy(&OBJ(c, i, 0, 0, 0), lo + i * pl, pl * sizeof(xo_real));
+    if (hi) memcpy(&OBJ(c, i, c->N_z + 1, 0, 0), hi + i * pl, pl * sizeof(xo_real));
+  }
 }
 
 /* ------------------------------------------------------ voxel update ----- */
@@ -691,7 +720,8 @@ static xo_real xo_update_voxels(xo_ctx *c, int32_t i, int32_t zb, int32_t ze, in
   xo_real *av = (xo_real *)calloc((size_t)(maxv ? maxv : 1) * c->amax, sizeof(xo_real));
   int32_t *ai = (int32_t *)calloc((size_t)(maxv ? maxv : 1) * c->amax, 4);
   int32_t *ac = (int32_t *)calloc((size_t)(maxv ? maxv : 1), 4);
-  const int32_t zmin = 1, zmax = c->N_z;
+  /* a rank reads the halo slices of its neighbours, XT_VoxUpdate.c:94-99 */
+  const int32_t zmin = c->slab_lo ? 0 : 1, zmax = c->slab_hi ? c->N_z + 1 : c->N_z;
   for (int32_t ix = xyb; ix <= xye; ix++) {
     int32_t k = xs[ix], j = ys[ix];
     mag[(size_t)j * c->N_x + k] = 0;

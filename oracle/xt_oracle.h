@@ -82,6 +82,10 @@ void xo_forward_project(const xo_ctx *c, xo_real *ax /*[N_p][N_r][N_t]*/);
 void xo_init_error_sino(xo_ctx *c);
 /* e = y - delta_t A x - d (the voxel update's matrix; see xt_oracle.c) */
 void xo_init_error_sino_model(xo_ctx *c);
+/* z slab of a volume split over ranks (see xt_oracle.c) */
+void xo_set_slab(xo_ctx *c, int32_t below, int32_t above);
+void xo_get_boundary(const xo_ctx *c, xo_real *lo, xo_real *hi);
+void xo_set_halo(xo_ctx *c, const xo_real *lo, const xo_real *hi);
 /* MAP cost of the object with FP64 sums (see xt_oracle.c) */
 double xo_map_cost_fp64(const xo_ctx *c, double *fwd, double *prior);
 xo_real xo_cost(xo_ctx *c, xo_real *forward, xo_real *prior);

@@ -14,8 +14,8 @@ zingers):
     lower in cost, so the fallback keeps the multi-resolution start;
   * a network trained on 16 phantoms reconstructed by the engine lowers the
     MAP cost of a held-out phantom's start below the multi-resolution start
-    it was given, and needs no more iterations than it to reach
-    (1 + 1e-3) of the converged cost.
+    it was given, and needs strictly fewer iterations than it to reach
+    (1 + 1e-4) of the converged cost.
 """
 import os
 import sys
@@ -150,10 +150,14 @@ def test_untrained_network_falls_back_to_multires_start():
 
 
 def test_trained_network_lowers_start_cost():
+    """What the network gains over the method without it: on a held-out
+    phantom its start needs strictly fewer fine iterations than the
+    multi-resolution start it refines to reach MAP cost <= (1 + 1e-4) of the
+    converged cost (the benchmark's tolerance)."""
     data, shape = tw.make_set(16, N, NT, NP, coarse_iters=20, target_iters=40, seed=500, log=lambda *a: None)
     net, losses = tw.train(data, shape, steps=400, batch=8, patch=(32, 32, 16), log=lambda *a: None)
     assert losses[-50:].mean() < losses[:50].mean()
-    target = converged() * (1 + 1e-3)
+    target = converged() * (1 + 1e-4)
     c = held_out_ctx()
     used, cn, ci = c.init_learned(net, 20)
     assert used and cn < ci, (cn, ci)
@@ -161,6 +165,6 @@ def test_trained_network_lowers_start_cost():
     c = held_out_ctx()
     c.init_multires(20)
     n_multi = iters_to(c, 1, target)
-    print("iterations to 1e-3: learned", n_learned, "multires", n_multi, "start costs", cn, ci)
-    assert n_learned is not None and n_multi is not None and n_learned <= n_multi
+    print("iterations to 1e-4: learned", n_learned, "multires", n_multi, "start costs", cn, ci)
+    assert n_learned is not None and n_multi is not None and n_learned < n_multi
     net.close()

@@ -105,6 +105,13 @@ struct xtg_ctx {
   xtg_ctx *coarse = nullptr;      // multi-resolution start: the 2x coarser grid
   int coarse_flags = 0;           // the XTG_MULTIRES_* flags it was built for
   int zslab_req = 0;  // z slices per ICD work piece; 0 = from the L2 size
+  // z slab of a volume split over processes (xtg_set_slab): caller-owned
+  // device planes [N_time][N_y][N_x] and the exchange hook
+  float *send_lo = nullptr, *send_hi = nullptr;
+  const float *halo_lo = nullptr, *halo_hi = nullptr;
+  xtg_exchange_fn xfn = nullptr;
+  void *xuser = nullptr;
+  int xphase = 0;
   cudaStream_t st = nullptr;
   cudaStream_t st_copy = nullptr;               // host-to-device copies that overlap the projector
   cudaEvent_t ev_y = nullptr, ev_w = nullptr;  // ... and their completion on it
@@ -177,7 +184,10 @@ __global__ void k_amatrix_batch(DevGeo G, const float *hr, const float *cosv, co
 }
 
 // qGGMRF prior over forward neighbour pairs (XT_ICD_update.c:202-294), FP64.
-__global__ void k_prior_cost64(DevGeo G, const float *x, double *slots) {
+// halo_hi (z slab with a neighbour above): the pairs from the top slice into
+// that neighbour's bottom slice belong to this slab's sum, as the reference's
+// ranks other than the last include Object[i][N_z+1] (XT_ICD_update.c:203-205).
+__global__ void k_prior_cost64(DevGeo G, const float *x, const float *halo_hi, double *slots) {
   const size_t n = (size_t)G.N_time * G.N_y * G.N_x * G.N_z;
   double acc = 0.0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -190,11 +200,12 @@ __global__ void k_prior_cost64(DevGeo G, const float *x, double *slots) {
     const double v = x[i];
     const double sq = G.Sigma_S_Q, sqp = G.Sigma_S_Q_P, cs = G.C_S, pp = G.MRF_P;
     auto X = [&](int ff, int jj, int kk, int zz) -> double {
+      if (zz == G.N_z) return (double)halo_hi[((size_t)ff * G.N_y + jj) * G.N_x + kk];
       return (double)x[(((size_t)ff * G.N_y + jj) * G.N_x + kk) * G.N_z + zz];
     };
     auto term = [&](int dz, int dy, int dx) {
       const int jj = j + dy, kk = k + dx, zz = z + dz;
-      if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x || zz >= G.N_z) return;
+      if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x || (zz >= G.N_z && !halo_hi)) return;
       acc += (double)G.SF[(1 + dz) * 9 + (1 + dy) * 3 + (1 + dx)] * xt_qggmrf_value64(v - X(f, jj, kk, zz), sq, sqp, cs, pp);
     };
     term(0, 0, 1);
@@ -218,6 +229,16 @@ __global__ void k_prior_cost64(DevGeo G, const float *x, double *slots) {
 }
 
 // data term from the running e (XT_ICD_update.c:188-200), FP64 arithmetic.
+// boundary slices of this slab for its neighbours: lo = slice 0, hi = slice
+// N_z - 1, each [N_time][N_y][N_x]
+__global__ void k_slab_pack(DevGeo G, const float *x, float *lo, float *hi) {
+  const size_t n = (size_t)G.N_time * G.N_y * G.N_x;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    if (lo) lo[q] = x[q * G.N_z];
+    if (hi) hi[q] = x[q * G.N_z + G.N_z - 1];
+  }
+}
+
 __global__ void k_running_cost64(size_t n, const float *e, const float *w, float T, float delta, double *slots) {
   double acc = 0.0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -849,7 +870,31 @@ int xtg_get_hr(const xtg_ctx *c, float *hr) {
 
 static int choose_amode(xtg_ctx *c, int *mode);
 static int zslab(const xtg_ctx *c);
+static int slab_exchange(xtg_ctx *c);
 
+int xtg_set_slab(xtg_ctx *c, float *send_below, float *send_above, const float *recv_below, const float *recv_above,
+                 xtg_exchange_fn exchange, void *user) {
+  if (!c || (!send_below) != (!recv_below) || (!send_above) != (!recv_above) ||
+      ((send_below || send_above) && !exchange)) {
+    set_err("xtg_set_slab: each side needs both planes, and planes need an exchange hook");
+    return XTG_E_ARG;
+  }
+  if ((send_below || send_above) && (c->prm.do_VarEst || c->prm.updateProjOffset > 1)) {
+    set_err("xtg_set_slab: variance and offset re-estimation need sums over every slab; not supported for slabs");
+    return XTG_E_ARG;
+  }
+  c->send_lo = send_below;
+  c->send_hi = send_above;
+  c->halo_lo = recv_below;
+  c->halo_hi = recv_above;
+  c->xfn = (send_below || send_above) ? exchange : nullptr;
+  c->xuser = user;
+  return 0;
+}
+int xtg_slab_exchange(xtg_ctx *c) {
+  if (!c) return XTG_E_ARG;
+  return slab_exchange(c);
+}
 int xtg_get_zslab(const xtg_ctx *c, int32_t *slices) {
   if (!c || !slices) return XTG_E_ARG;
   *slices = zslab(c);
@@ -1378,7 +1423,7 @@ int xtg_resync_fp64(xtg_ctx *c, double *cost, double *fwd, double *prior) {
 static int finish_cost(xtg_ctx *c, double data_sum, double *cost, double *fwd, double *prior) {
   CK(cudaMemsetAsync(c->d_red + NSLOT, 0, NSLOT * 8, c->st));
   const unsigned grid = std::min<unsigned>(blocks_for(c->nvox, 256), (unsigned)c->sm_count * 8);
-  k_prior_cost64<<<grid, 256, 0, c->st>>>(c->G, c->d_x, c->d_red + NSLOT);
+  k_prior_cost64<<<grid, 256, 0, c->st>>>(c->G, c->d_x, c->halo_hi, c->d_red + NSLOT);
   c->launches++;
   CK(cudaGetLastError());
   double h[NSLOT];
@@ -1664,6 +1709,7 @@ static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, c
   A.tstart = c->d_tstart; A.toff = c->d_toff; A.tval32 = c->d_tval32; A.tval16 = c->d_tval16; A.tscale = c->d_tscale;
   A.T2 = g.T * g.T; A.Tdelta = g.T * g.delta; A.st_absx = c->d_absx; A.st_cnt = c->d_cnt; A.err = c->d_err;
   A.zslab = hz; A.nsub = nsub;
+  A.halo_lo = c->halo_lo; A.halo_hi = c->halo_hi;
   if (nsub > 1) {
     CK(launch_magmap_zero(c->G, A, c->sm_count * 4, c->st));
     c->launches++;
@@ -1814,6 +1860,29 @@ static float host_randomized_select(xtg_ctx *c, float *A, unsigned p, unsigned r
   }
 }
 
+// Halo exchange of a z slab (the reference's MPI_Send_Recv_Z_Slices /
+// MPI_Wait_Z_Slices after every half-pass, XT_MPI.c:47-122): this slab's
+// boundary slices go into the send planes, the stream is drained, and the
+// caller's hook moves them to the neighbours and fills the halo planes
+// before the next launch reads them.
+static int slab_exchange(xtg_ctx *c) {
+  if (!c->xfn) return 0;
+  if (c->send_lo || c->send_hi) {
+    const size_t n = (size_t)c->g.N_time * c->g.N_y * c->g.N_x;
+    k_slab_pack<<<std::min<unsigned>(blocks_for(n, 256), (unsigned)c->sm_count * 4), 256, 0, c->st>>>(
+        c->G, c->d_x, c->send_lo, c->send_hi);
+    c->launches++;
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->st));
+  const int rc = c->xfn(c->xuser, c->xphase++);
+  if (rc) {
+    set_err("slab halo exchange hook failed (%d)", rc);
+    return XTG_E_STATE;
+  }
+  return 0;
+}
+
 static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
   const long long icd0 = c->icd_launches;
   const xt_geom &g = c->g;
@@ -1850,6 +1919,7 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
     if (rc) return rc;
     CK(cudaEventRecord(c->tev[2 * ntimed + 1], c->st));
     ntimed++;
+    if ((rc = slab_exchange(c))) return rc;
     if (j == K - 1) {
       rc = read_stats(c, st, &vox_mag);
       if (rc) return rc;
@@ -1870,6 +1940,7 @@ static int icd_iteration_parallel(xtg_ctx *c, int iter, xtg_stats *st) {
         if (rc) return rc;
         CK(cudaEventRecord(c->tev[2 * ntimed + 1], c->st));
         ntimed++;
+        if ((rc = slab_exchange(c))) return rc;
         if (c->prm.updateProjOffset > 1) {
           rc = xtg_update_offset(c);
           if (rc) return rc;
@@ -2021,6 +2092,9 @@ int xtg_icd_iteration(xtg_ctx *c, int32_t iter, xtg_stats *st_out) {
   memset(&st, 0, sizeof(st));
   int rc = reset_stats(c);
   if (rc) return rc;
+  // a slab starts every iteration from its neighbours' current boundary slices
+  c->xphase = 0;
+  if ((rc = slab_exchange(c))) return rc;
   CK(cudaEventRecord(c->ev0, c->st));
   rc = (c->order == XTG_ORDER_SEQUENTIAL) ? icd_iteration_sequential(c, iter, &st) : icd_iteration_parallel(c, iter, &st);
   if (rc) return rc;

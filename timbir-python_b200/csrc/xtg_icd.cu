@@ -74,14 +74,16 @@ struct Nbr {
   float b;  // filter weight * surrogate coefficient, 0 when the slot is absent
 };
 
+// hlo / hhi: the slices below slice 0 and above slice N_z - 1 belong to a
+// neighbouring slab (their values are staged in sNb like any other)
 __device__ __forceinline__ Nbr nbr_term(const DevGeo &G, const float *sNb, const float *sTn, int zmax, int z, int zb,
-                                        int fr, int row, int col, float Vv, int n) {
+                                        int fr, int row, int col, float Vv, int n, bool hlo, bool hhi) {
   Nbr o{0.f, 0.f};
   if (n < 27) {
     if (n == 13) return o;
     const int dz = n / 9, c = n % 9;
     const int za = zb + z + dz - 1;
-    if (za < 0 || za >= G.N_z) return o;
+    if ((za < 0 && !hlo) || (za >= G.N_z && !hhi)) return o;
     const int jj = row + c / 3 - 1, kk = col + c % 3 - 1;
     if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x) return o;
     o.v = sNb[c * (zmax + 2) + z + dz];
@@ -122,6 +124,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nitems = A.n_items_dev ? *A.n_items_dev : A.n_items;
+  const bool hlo = A.halo_lo != nullptr, hhi = A.halo_hi != nullptr;
 
   for (;;) {
     if (tid == 0) {
@@ -151,14 +154,24 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     const int V = A.view_num[fr], vs = A.view_start[fr];
 
     // 1. neighbourhood: the 3x3 columns' z-lines over [zb-1, ze+1], and the
-    //    same column in frames fr-1 and fr+1 (0 outside the volume)
+    //    same column in frames fr-1 and fr+1 (0 outside the volume; slices
+    //    -1 and N_z from the neighbouring slabs' halo planes when present,
+    //    as the reference's ranks read Object[i][0] / [N_z+1],
+    //    XT_VoxUpdate.c:94-99)
     const size_t plane = (size_t)G.N_y * G.N_x;
     for (int k = tid; k < 9 * (Z + 2); k += NT) {
       const int c = k / (Z + 2), zz = k - c * (Z + 2);
       const int jj = row + c / 3 - 1, kk = col + c % 3 - 1, za = zb - 1 + zz;
       float v = 0.f;
-      if (jj >= 0 && jj < G.N_y && kk >= 0 && kk < G.N_x && za >= 0 && za < G.N_z)
-        v = A.x[(((size_t)fr * plane) + (size_t)jj * G.N_x + kk) * G.N_z + za];
+      if (jj >= 0 && jj < G.N_y && kk >= 0 && kk < G.N_x) {
+        const size_t q = (size_t)fr * plane + (size_t)jj * G.N_x + kk;
+        if (za >= 0 && za < G.N_z)
+          v = A.x[q * G.N_z + za];
+        else if (za < 0 && hlo)
+          v = A.halo_lo[q];
+        else if (za >= G.N_z && hhi)
+          v = A.halo_hi[q];
+      }
       sNb[c * (zmax + 2) + zz] = v;
     }
     for (int k = tid; k < 2 * Z; k += NT) {
@@ -376,7 +389,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
           }
           float num = 0.f, den = 0.f;
           for (int n = 0; n < 29; n++) {
-            const Nbr o = nbr_term(G, sNb, sTn, zmax, z, zb, fr, row, col, Vv, n);
+            const Nbr o = nbr_term(G, sNb, sTn, zmax, z, zb, fr, row, col, Vv, n, hlo, hhi);
             num += o.b * o.v;
             den += o.b;
           }
@@ -413,7 +426,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
           for (int k = 0; k < 4; k++) {
             const int n = sub + 8 * k;
             if (n < 29) {
-              const Nbr o = nbr_term(G, sNb, sTn, zmax, z, zb, fr, row, col, Vv, n);
+              const Nbr o = nbr_term(G, sNb, sTn, zmax, z, zb, fr, row, col, Vv, n, hlo, hhi);
               num += o.b * o.v;
               den += o.b;
             }

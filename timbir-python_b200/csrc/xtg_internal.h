@@ -33,6 +33,9 @@ struct IcdArgs {
   int n_masked;
   int iter;
   float T2, Tdelta;
+  // z slab of a larger volume: the neighbouring slabs' boundary slices,
+  // [N_time][N_y][N_x] (null where this slab ends the volume)
+  const float *halo_lo, *halo_hi;
   double *st_absx;             // [64] slots
   unsigned long long *st_cnt;  // [0] voxel updates, [1] zero skipped, [2] items
   int *err;

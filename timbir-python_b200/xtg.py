@@ -27,7 +27,7 @@ XTG_PROJ_AUTO, XTG_PROJ_GATHER, XTG_PROJ_TABLE = 0, 1, 2
 
 # symbols declared in include/xtg.h and include/xt_gen.h
 XTG_SYMBOLS = [
-    "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_init_object_fbp", "xtg_object_to_device",
+    "xtg_create", "xtg_destroy", "xtg_set_zslab", "xtg_set_slab", "xtg_slab_exchange", "xtg_init_object_fbp", "xtg_object_to_device",
     "xtg_object_from_device", "xtg_upsample", "xtg_init_object_multires", "xtg_get_zslab", "xtg_last_error", "xtg_abi_version", "xtg_dims", "xtg_geometry",
     "xtg_get_hr", "xtg_set_options", "xtg_get_options", "xtg_set_projector", "xtg_get_projector", "xtg_upload_sino", "xtg_upload_sino_start", "xtg_upload_counts", "xtg_upload_object",
     "xtg_download_object", "xtg_get_error_sino", "xtg_set_error_sino", "xtg_get_weight",
@@ -321,6 +321,30 @@ class Context:
         _check(self.lib.xtg_init_object_learned(self.h, net.h, int(coarse_iters), C.byref(used), C.byref(cn),
                                                 C.byref(ci)), "xtg_init_object_learned")
         return bool(used.value), cn.value, ci.value
+
+    # the exchange hook's C type: int (*)(void *user, int32_t phase)
+    EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32)
+
+    def set_slab(self, send_below, send_above, recv_below, recv_above, exchange):
+        """This context is one z slab of a larger volume (xtg_set_slab): device
+        planes [N_time][N_y][N_x] (torch CUDA tensors or None per side) and
+        exchange(phase) -> None, called whenever the neighbours' slices are
+        due; it must fill recv_* from the neighbours' send_* before it
+        returns."""
+        def hook(user, phase):
+            try:
+                exchange(int(phase))
+                return 0
+            except Exception as err:  # reported through the library's error path
+                self._hook_error = err
+                return 1
+        self._hook = self.EXCHANGE_FN(hook)  # kept alive as long as the context uses it
+        self._slab_planes = (send_below, send_above, recv_below, recv_above)
+        ptr = [None if t is None else C.c_void_p(t.data_ptr()) for t in self._slab_planes]
+        _check(self.lib.xtg_set_slab(self.h, ptr[0], ptr[1], ptr[2], ptr[3], self._hook, None), "xtg_set_slab")
+
+    def slab_exchange(self):
+        _check(self.lib.xtg_slab_exchange(self.h), "xtg_slab_exchange")
 
     def set_zslab(self, slices):
         _check(self.lib.xtg_set_zslab(self.h, int(slices)), "xtg_set_zslab")
