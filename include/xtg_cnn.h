@@ -49,6 +49,14 @@ int xtc_conv3d_wgrad(const void *in, const void *dout, float *dw, int32_t nb, in
  * each, the engine's device layout with nb = frames); output: start image +
  * correction (the `icd` argument below is the start image).  Y, X, Z must be multiples of 8.  About 1.44 M
  * FP32 master parameters; BF16 weights and activations, FP32 accumulation. */
+/* Health check of the bounded waits the tensor-core kernels use on their
+ * mbarriers: one CTA waits `polls` polls on a barrier that it has arrived on
+ * (arrive != 0: returns 0) or that nothing will complete (arrive == 0: the
+ * wait gives up, sets the device error flag, and the call returns
+ * XTG_E_TIMEOUT; nothing is in flight, the context stays usable).  No
+ * reference counterpart. */
+int xtc_wait_selftest(int32_t arrive, int64_t polls);
+
 typedef struct xtc_net xtc_net;
 
 /* He-initialised weights from the seed; the head starts at zero, so the new

@@ -42,6 +42,19 @@ int ensure_err() {
 
 extern "C" {
 
+int xtc_wait_selftest(int32_t arrive, int64_t polls) {
+  if (polls < 1) {
+    xtg_set_error_text("xtc_wait_selftest: polls must be positive");
+    return XTG_E_ARG;
+  }
+  int rc = ensure_err();
+  if (rc) return rc;
+  cudaError_t e = xtc::wait_selftest(arrive != 0, (long long)polls, g_err, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(e, "xtc_wait_selftest");
+  return check_err_flag("xtc_wait_selftest");
+}
+
 int xtc_conv3d_path(const void *in, const void *w, const float *bias, void *out, int32_t nb, int32_t Y, int32_t X,
                     int32_t Z, int32_t cin, int32_t cout, int32_t kpad, int32_t epi, int32_t sign, int32_t path) {
   if (!in || !w || !out || (epi == 0 && !bias) || epi < 0 || epi > 2 || (sign != 1 && sign != -1) ||

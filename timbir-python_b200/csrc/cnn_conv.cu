@@ -31,8 +31,8 @@ __device__ __forceinline__ void tap_offset(int tap, int &dy, int &dx, int &dz) {
 }
 
 // Block-uniform bounded wait; on timeout sets *err and returns false.
-__device__ __forceinline__ bool wait_stage(uint64_t *mbar, uint32_t parity, int *err) {
-  const bool ok = mbar_wait(mbar, parity, 1ll << 24);
+__device__ __forceinline__ bool wait_stage(uint64_t *mbar, uint32_t parity, int *err, long long limit = 1ll << 24) {
+  const bool ok = mbar_wait(mbar, parity, limit);
   const bool all = __syncthreads_and(ok) != 0;
   if (!all && threadIdx.x == 0) atomicExch(err, 1);
   return all;
@@ -470,6 +470,26 @@ cudaError_t conv_first(int nb, int Y, int X, int Z, const float *a, const float 
   if (e != cudaSuccess) return e;
   k_conv_first<<<(unsigned)((M + 127) / 128), CONV_THREADS, smem, st>>>(nb, Y, X, Z, a, b, scale, w64, bias, n, out,
                                                                          err);
+  return cudaGetLastError();
+}
+
+// The bounded-wait path of the tensor-core kernels exercised alone: one CTA
+// waits on a fresh mbarrier (count 1) with `limit` polls, after thread 0
+// has arrived on it or not.  Nothing is in flight, so a wait that gives up
+// leaves nothing behind; it sets *err like a convolution's would.
+__global__ void k_wait_selftest(int arrive, long long limit, int *err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (arrive && threadIdx.x == 0) mbar_arrive(&bar);
+  wait_stage(&bar, 0, err, limit);
+}
+
+cudaError_t wait_selftest(int arrive, long long limit, int *err, cudaStream_t st) {
+  k_wait_selftest<<<1, 128, 0, st>>>(arrive, limit, err);
   return cudaGetLastError();
 }
 

@@ -51,4 +51,5 @@ void adam(long long n, float *p, const float *g, float *m, float *v, float lr, f
 void crop(int np, const float *const *src, const int4 *org, int Y, int X, int Z, int py, int px, int pz, float *dst,
           cudaStream_t st);
 
+cudaError_t wait_selftest(int arrive, long long limit, int *err, cudaStream_t st);
 }  // namespace xtc
