@@ -239,15 +239,34 @@ __global__ void k_slab_pack(DevGeo G, const float *x, float *lo, float *hi) {
   }
 }
 
+// generalized-Huber data term of one entry (XT_ICD_update.c:192-198), FP64
+__device__ __forceinline__ double huber_term(float e, float w, double T, double delta) {
+  const double s = (double)e * sqrt((double)w);
+  return fabs(s) < T ? s * s : 2.0 * delta * T * fabs(s) + T * T * (1.0 - 2.0 * delta);
+}
+
+// Data term of the running e (FP64 sums).  n4 = n / 4 entries are read as
+// float4 (16-byte loads, two in flight per thread), the rest one by one.
 __global__ void k_running_cost64(size_t n, const float *e, const float *w, float T, float delta, double *slots) {
+  const double Td = T, dd = delta;
   double acc = 0.0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const double s = (double)e[i] * sqrt((double)w[i]);
-    if (fabs(s) < (double)T)
-      acc += s * s;
-    else
-      acc += 2.0 * (double)delta * (double)T * fabs(s) + (double)T * (double)T * (1.0 - 2.0 * (double)delta);
+  const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+  const float4 *e4 = reinterpret_cast<const float4 *>(e), *w4 = reinterpret_cast<const float4 *>(w);
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + stride < n4; i += 2 * stride) {
+    const float4 ea = __ldcs(e4 + i), wa = __ldcs(w4 + i), eb = __ldcs(e4 + i + stride), wb = __ldcs(w4 + i + stride);
+    acc += huber_term(ea.x, wa.x, Td, dd) + huber_term(ea.y, wa.y, Td, dd) + huber_term(ea.z, wa.z, Td, dd) +
+           huber_term(ea.w, wa.w, Td, dd);
+    acc += huber_term(eb.x, wb.x, Td, dd) + huber_term(eb.y, wb.y, Td, dd) + huber_term(eb.z, wb.z, Td, dd) +
+           huber_term(eb.w, wb.w, Td, dd);
   }
+  for (; i < n4; i += stride) {
+    const float4 ea = __ldcs(e4 + i), wa = __ldcs(w4 + i);
+    acc += huber_term(ea.x, wa.x, Td, dd) + huber_term(ea.y, wa.y, Td, dd) + huber_term(ea.z, wa.z, Td, dd) +
+           huber_term(ea.w, wa.w, Td, dd);
+  }
+  for (size_t q = 4 * n4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
+    acc += huber_term(e[q], w[q], Td, dd);
   __shared__ double red[32];
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
@@ -259,13 +278,27 @@ __global__ void k_running_cost64(size_t n, const float *e, const float *w, float
   }
 }
 
-// ProjSelect = |e sqrt(w)| < T, in double like the reference's mixed expression.
+// ProjSelect = |e sqrt(w)| < T, in double like the reference's mixed
+// expression; float4 loads for the first n / 4 * 4 entries.
+__device__ __forceinline__ unsigned char zsel(float e, float w, double T) {
+  return (fabs((double)e * sqrt((double)w)) < T) ? 1 : 0;
+}
 __global__ void k_zinger_refresh(size_t n, const float *e, const float *w, float T, unsigned char *sel,
                                  unsigned long long *count) {
+  const double Td = T;
   unsigned c = 0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const unsigned char s = (fabs((double)e[i] * sqrt((double)w[i])) < (double)T) ? 1 : 0;
-    if (sel) sel[i] = s;
+  const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+  const float4 *e4 = reinterpret_cast<const float4 *>(e), *w4 = reinterpret_cast<const float4 *>(w);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const float4 ea = __ldcs(e4 + i), wa = __ldcs(w4 + i);
+    const unsigned char s0 = zsel(ea.x, wa.x, Td), s1 = zsel(ea.y, wa.y, Td), s2 = zsel(ea.z, wa.z, Td),
+                        s3 = zsel(ea.w, wa.w, Td);
+    if (sel) reinterpret_cast<uchar4 *>(sel)[i] = make_uchar4(s0, s1, s2, s3);
+    c += s0 + s1 + s2 + s3;
+  }
+  for (size_t q = 4 * n4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const unsigned char s = zsel(e[q], w[q], Td);
+    if (sel) sel[q] = s;
     c += s;
   }
   for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);

@@ -125,10 +125,29 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nitems = A.n_items_dev ? *A.n_items_dev : A.n_items;
   const bool hlo = A.halo_lo != nullptr, hhi = A.halo_hi != nullptr;
+  // Short items (small CTAs) are taken GRAB at a time and the CTA's
+  // statistics are added up in thread 0 and flushed once at the end: with
+  // tens of thousands of items per launch, per-item atomics on the same few
+  // addresses would queue at L2.
+  // (kept in shared memory: registers are the kernel's occupancy limit)
+  constexpr int GRAB = NT < XTG_THREADS ? 8 : 1;
+  __shared__ int sGrab[2];                 // base, next of the batch
+  __shared__ double sCtaAbs;
+  __shared__ unsigned long long sCta[3];   // voxel updates, zero skipped, items
+  if (tid == 0) {
+    sGrab[0] = 0;
+    sGrab[1] = GRAB;
+    sCtaAbs = 0.0;
+    sCta[0] = sCta[1] = sCta[2] = 0;
+  }
 
   for (;;) {
     if (tid == 0) {
-      sItem = atomicAdd(A.counter, 1);
+      if (sGrab[1] == GRAB) {
+        sGrab[0] = atomicAdd(A.counter, GRAB);
+        sGrab[1] = 0;
+      }
+      sItem = sGrab[0] + sGrab[1]++;
       sUpd = 0;
       sZero = 0;
     }
@@ -505,10 +524,10 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     if (tid == 0) {
       double s = 0.0;
       for (int wq = 0; wq < NT / 32; wq++) s += sAbs[wq];
-      atomicAdd(&A.st_absx[blockIdx.x & 63], s);
-      atomicAdd(&A.st_cnt[0], (unsigned long long)sUpd);
-      atomicAdd(&A.st_cnt[1], (unsigned long long)sZero);
-      if (piece == 0) atomicAdd(&A.st_cnt[2], 1ull);
+      sCtaAbs += s;
+      sCta[0] += sUpd;
+      sCta[1] += sZero;
+      if (piece == 0) sCta[2]++;
     }
 
     // 6. e -= (A delta_t) * delta_x on the footprint (XT_VoxUpdate.c:62-82)
@@ -549,6 +568,12 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
       }
     }
     __syncthreads();
+  }
+  if (tid == 0 && sCta[2]) {
+    atomicAdd(&A.st_absx[blockIdx.x & 63], sCtaAbs);
+    atomicAdd(&A.st_cnt[0], sCta[0]);
+    atomicAdd(&A.st_cnt[1], sCta[1]);
+    atomicAdd(&A.st_cnt[2], sCta[2]);
   }
 }
 
