@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     }
     __syncthreads();
   }
-  if (tid == 0 && sCta[2]) {
+  if (tid == 0 && (sCta[0] || sCta[1] || sCta[2] || sCtaAbs != 0.0)) {  // pieces past the first count no item
     atomicAdd(&A.st_absx[blockIdx.x & 63], sCtaAbs);
     atomicAdd(&A.st_cnt[0], sCta[0]);
     atomicAdd(&A.st_cnt[1], sCta[1]);
