@@ -352,7 +352,8 @@ def network_forward(nxy, nz, reps, weights=WEIGHTS):
     net.close()
 
 
-def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, coarse_iters=30, learned=True):
+def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, coarse_iters=30, learned=True,
+             weights=WEIGHTS, starts=("zero", "fbp", "multires", "learned")):
     """Seconds to MAP cost <= (1 + tol) C* from four starts:
       zero     -- the reference's start, plain ICD with the benchmark's A storage;
       fbp      -- the FBP image, same A storage;
@@ -396,9 +397,9 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
                             "own converged cost (tests/test_config_c2_pinned.py)",
            "_x_star": x_star}
     net = None
-    if learned and os.path.exists(WEIGHTS) and all(d % 8 == 0 for d in (ctx.N_x, ctx.N_y, ctx.N_z)):
+    if learned and "learned" in starts and os.path.exists(weights) and all(d % 8 == 0 for d in (ctx.N_x, ctx.N_y, ctx.N_z)):
         net = xtg.WarmNet()
-        net.load(WEIGHTS)
+        net.load(weights)
         # the network's activation buffers and the start images for this
         # volume are allocated once, outside the timed region (like the A table
         # and the coarse context): one learned start with a single coarse
@@ -407,7 +408,7 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     # the coarse context of the multi-resolution start is built once, outside
     # the timed region (like the fine context and its A table)
     ctx.init_multires(1)
-    runs = [("zero", AMODES[amode]), ("fbp", AMODES[amode]), ("multires", AMODES[amode])]
+    runs = [(k, AMODES[amode]) for k in ("zero", "fbp", "multires") if k in starts]
     if net is not None:
         runs.append(("learned", xtg.XTG_A_FP16))
     for kind, am in runs:
@@ -448,7 +449,7 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
         out["network"] = network_roofline(ctx, net, coarse_iters)
         net.close()
     ctx.set_options(a_mode=AMODES[amode])
-    z = out["zero"].get("s")
+    z = out.get("zero", {}).get("s")
     for k in ("fbp", "multires", "learned"):
         v = out.get(k, {}).get("s")
         out[f"speedup_{k}_vs_zero"] = z / v if z and v else None
@@ -600,7 +601,8 @@ def run_ours(args):
     if not args.no_converge and world == 1:
         # a single-GPU metric: with N replicas every rank would repeat it.
         # The committed warm-start weights were trained for the plain-3D geometry
-        line["time_to_cost"] = converge(ctx, args.amode, learned=args.workload == "plain3d" and not args.nxy)
+        line["time_to_cost"] = converge(ctx, args.amode, learned=args.workload == "plain3d" and not args.nxy,
+                                        weights=args.weights, starts=tuple(args.starts.split(",")))
         x_star = line["time_to_cost"].pop("_x_star")
         # the reference's CPU-runnable configuration, to its own FP64 converged cost
         line["time_to_cost_config1"] = config1_gpu(args.amode)
@@ -903,6 +905,9 @@ def main():
                     help="time the non-ICD kernels of the engine on the workload (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-other", action="store_true", help="skip the 4D workloads after the headline one")
+    ap.add_argument("--weights", default=WEIGHTS, help="warm-start network weights for the learned start")
+    ap.add_argument("--starts", default="zero,fbp,multires,learned",
+                    help="starts timed by time_to_cost (comma-separated subset)")
     ap.add_argument("--no-converge", action="store_true", help="skip the seconds-to-converged-cost run")
     args = ap.parse_args()
     if args.network_forward:
