@@ -35,6 +35,7 @@ struct Layer {
   size_t off_w, off_b;  // offsets in the parameter vector
   bf16 *W = nullptr, *Wt = nullptr;
   bf16 *Wp = nullptr;   // W packed for the tile kernel
+  bf16 *Wtp = nullptr;  // Wt packed for the tile kernel (input gradient, layers with cin <= 64)
   bf16 *W64 = nullptr;  // the first layer's W as [cout][64], k = 2 tap + channel
 };
 
@@ -108,6 +109,7 @@ int pack_all(xtc_net *n) {
     Layer &l = n->L[i];
     xtc::pack_weights(l.cin_real, l.cin, l.cout, l.kpad, l.kpad_t, n->P + l.off_w, l.W, i ? l.Wt : nullptr, n->st);
     if (l.Wp) NCK(xtc::conv_tile_pack(l.cin, l.cout, l.kpad, 1, l.W, l.Wp, n->st));
+    if (l.Wtp) NCK(xtc::conv_tile_pack(l.cout, l.cin, l.kpad_t, -1, l.Wt, l.Wtp, n->st));
     if (l.W64) NCK(xtc::conv_first_pack(l.cout, l.cin, l.kpad, l.W, l.W64, n->st));
   }
   NCK(cudaGetLastError());
@@ -229,7 +231,17 @@ int conv_back(xtc_net *n, int li, const float *dpost, const bf16 *post, const bf
     xtc::fold_wgrad(l.cin_real, l.cin, l.cout, n->graw, n->G + l.off_w, n->st);
   }
   if (din) {
+    // the input gradient: the same convolution with transposed weights and
+    // negated offsets, on the tile kernel where the shape allows
     xtc::ConvShape t{n->nb, n->Y >> lvl, n->X >> lvl, n->Z >> lvl, l.cout, l.cin, l.kpad_t};
+    if (l.Wtp && xtc::conv_tile_supported(t)) {
+      const cudaError_t e = xtc::conv_forward_tile(t, dpre, l.Wtp, nullptr, din, 2, -1, n->d_err, n->st);
+      if (e != cudaErrorNotSupported) {
+        NCK(e);
+        return 0;
+      }
+      cudaGetLastError();
+    }
     NCK(xtc::conv_forward(t, dpre, l.Wt, nullptr, din, 2, -1, n->d_err, n->st));
   }
   return 0;
@@ -331,6 +343,7 @@ int xtc_net_create(uint64_t seed, xtc_net **out) {
     A((void **)&l.W, (size_t)l.cout * l.kpad * 2);
     if (i) A((void **)&l.Wt, (size_t)l.cin * l.kpad_t * 2);
     if (l.cout <= 64) A((void **)&l.Wp, xtc::conv_tile_wp_elems(l.cin, l.cout) * 2);
+    if (i && l.cin <= 64 && l.cin % 16 == 0) A((void **)&l.Wtp, xtc::conv_tile_wp_elems(l.cout, l.cin) * 2);
     if (i == 0) A((void **)&l.W64, (size_t)l.cout * 64 * 2);
   }
   if (e == cudaSuccess) e = cudaMemcpy(n->P, h.data(), off * 4, cudaMemcpyHostToDevice);
@@ -356,6 +369,7 @@ void xtc_net_destroy(xtc_net *n) {
     if (n->L[i].W) cudaFree(n->L[i].W);
     if (n->L[i].Wt) cudaFree(n->L[i].Wt);
     if (n->L[i].Wp) cudaFree(n->L[i].Wp);
+    if (n->L[i].Wtp) cudaFree(n->L[i].Wtp);
     if (n->L[i].W64) cudaFree(n->L[i].W64);
   }
   delete n;

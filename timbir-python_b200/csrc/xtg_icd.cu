@@ -29,6 +29,18 @@ namespace xtg {
 #ifndef XTG_SMALL_NT
 #define XTG_SMALL_NT 64
 #endif
+// Longer items whose column runs hold at most XTG_MEDIUM_ENTRIES A entries
+// run in CTAs of XTG_MEDIUM_NT threads (table modes, parallel schedule): the
+// per-item fixed work weighs more when the footprint is short, and twice as
+// many CTAs per SM overlap it better.  The largest 4D volume (352 entries
+// per column and frame): 745 -> 888 M voxel updates/s; 64 threads: equal;
+// plain 3D (2195 entries) in 128-thread CTAs: 221 against 241 M.
+#ifndef XTG_MEDIUM_ENTRIES
+#define XTG_MEDIUM_ENTRIES 1024
+#endif
+#ifndef XTG_MEDIUM_NT
+#define XTG_MEDIUM_NT 128
+#endif
 
 // Footprint loads with L2 cache hints: e (re-read and updated through L2 by
 // other columns' reductions) is kept (evict_last), w (read once per visit) is
@@ -601,7 +613,8 @@ static IcdKernel icd_kernel(int vec, int amode, int seq, int as, int nt) {
 #define XTG_K(V, S) (as == 3 ? k_icd_columns<V, 0, S, 3> : as == 4 ? k_icd_columns<V, 0, S, 4> : k_icd_columns<V, 0, S, 12>)
 #define XTG_T(V, M, S) k_icd_columns<V, M, S, 3>
   if (nt != XTG_THREADS && vec == 4 && amode != 0 && !seq)  // short items, table modes
-    return amode == 1 ? k_icd_columns<4, 1, 0, 3, XTG_SMALL_NT> : k_icd_columns<4, 2, 0, 3, XTG_SMALL_NT>;
+    return nt == XTG_SMALL_NT ? (amode == 1 ? k_icd_columns<4, 1, 0, 3, XTG_SMALL_NT> : k_icd_columns<4, 2, 0, 3, XTG_SMALL_NT>)
+                              : (amode == 1 ? k_icd_columns<4, 1, 0, 3, XTG_MEDIUM_NT> : k_icd_columns<4, 2, 0, 3, XTG_MEDIUM_NT>);
   if (vec == 4) {
     if (amode == 0) return seq ? XTG_K(4, 1) : XTG_K(4, 0);
     if (amode == 1) return seq ? XTG_T(4, 1, 1) : XTG_T(4, 1, 0);
@@ -634,14 +647,16 @@ cudaError_t launch_magmap_zero(const DevGeo &G, const IcdArgs &A, int grid, cuda
 }
 
 // threads per CTA for items of zmax slices: XTG_SMALL_NT for short table-mode items
-int icd_threads(int vec, int amode, int seq, int zmax, int zovl) {
-  return (vec == 4 && amode != 0 && !seq && zmax * zovl <= XTG_SMALL_ROWS) ? XTG_SMALL_NT : XTG_THREADS;
+int icd_threads(int vec, int amode, int seq, int zmax, int zovl, int vmax) {
+  if (vec == 4 && amode != 0 && !seq && zmax * zovl <= XTG_SMALL_ROWS) return XTG_SMALL_NT;
+  if (vec == 4 && amode != 0 && !seq && vmax <= XTG_MEDIUM_ENTRIES) return XTG_MEDIUM_NT;
+  return XTG_THREADS;
 }
 
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st) {
   const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as, amode, vec);
-  const int nt = icd_threads(vec, amode, seq, zmax, G.zovl);
+  const int nt = icd_threads(vec, amode, seq, zmax, G.zovl, vmax);
   IcdKernel k = icd_kernel(vec, amode, seq, as, nt);
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -656,7 +671,7 @@ cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, in
 
 int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl) {
   const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as, amode, vec);
-  const int nt = icd_threads(vec, amode, seq, zmax, zovl);
+  const int nt = icd_threads(vec, amode, seq, zmax, zovl, vmax);
   IcdKernel k = icd_kernel(vec, amode, seq, as, nt);
   int nb = 0;
   cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -96,16 +96,19 @@ def main():
     ap.add_argument("--views", type=int, default=512)
     ap.add_argument("--coarse-iters", type=int, default=30)
     ap.add_argument("--target-iters", type=int, default=40)
+    ap.add_argument("--patch", type=int, nargs=3, default=(64, 64, 32), metavar=("Y", "X", "Z"),
+                    help="training patch; X a multiple of 128 runs the level-0 convolutions (forward and input "
+                         "gradient) on the TMA tile kernel")
     args = ap.parse_args()
     t0 = time.time()
     data, shape = make_set(args.volumes, args.n, args.nt, args.views, coarse_iters=args.coarse_iters,
                            target_iters=args.target_iters)
     t1 = time.time()
-    net, losses = train(data, shape, steps=args.steps, batch=args.batch)
+    net, losses = train(data, shape, steps=args.steps, batch=args.batch, patch=tuple(args.patch))
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     net.save(args.out)
     info = {"volumes": args.volumes, "shape": shape, "views": args.views, "coarse_iters": args.coarse_iters,
-            "target_iters": args.target_iters, "steps": args.steps, "batch": args.batch,
+            "target_iters": args.target_iters, "steps": args.steps, "batch": args.batch, "patch": list(args.patch),
             "data_s": t1 - t0, "train_s": time.time() - t1, "loss_first50": float(losses[:50].mean()),
             "loss_last50": float(losses[-50:].mean()), "params": net.n_params}
     with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
