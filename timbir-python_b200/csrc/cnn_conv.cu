@@ -83,10 +83,15 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv_tc(ConvShape s, const __n
     if (!ok) break;
     // A: this thread's row, 8 chunks of 8 K elements (one tap, 8 channels each)
     uint8_t *a = sA + st * A_STAGE;
+    // (tap, channel) of the stage's first chunk; the next chunks step 8
+    // channels (cin is a multiple of 8), so one division per stage
+    int tap = (kt * KT) / s.cin, ci = kt * KT - tap * s.cin;
 #pragma unroll
-    for (int c = 0; c < KT / 8; c++) {
-      const int k = kt * KT + c * 8;
-      const int tap = k / s.cin, ci = k - tap * s.cin;
+    for (int c = 0; c < KT / 8; c++, ci += 8) {
+      if (ci >= s.cin) {
+        ci -= s.cin;
+        tap++;
+      }
       int4 v = make_int4(0, 0, 0, 0);
       if (mval && tap < 27) {
         int dy, dx, dz;
@@ -228,17 +233,35 @@ __global__ void __launch_bounds__(CONV_THREADS) k_wgrad_tc(ConvShape s, const __
     uint8_t *a = sA + st * A_STAGE;
     {
       int4 ld[8], tr[8];
+      if (s.Z % 8 == 0) {
+        // the 8 voxels start at a multiple of 8 and lie on one z-line: one
+        // coordinate decode for the group
+        const long long v0 = vb + ca * 8;
+        int b = 0, yy = 0, xx = 0, zz = 0;
+        if (v0 < kend) voxel_coords(s, v0, b, yy, xx, zz);
+        const int y2 = yy + ddy, x2 = xx + ddx;
+        const bool line = ra < rows && y2 >= 0 && y2 < s.Y && x2 >= 0 && x2 < s.X;
+        const __nv_bfloat16 *base = line ? in + (((size_t)b * s.Y + y2) * s.X + x2) * s.Z * s.cin + ci : in;
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        ld[u] = make_int4(0, 0, 0, 0);
-        const long long v = vb + ca * 8 + u;
-        if (ra < rows && v < kend) {
-          int b, yy, xx, zz;
-          voxel_coords(s, v, b, yy, xx, zz);
-          const int y2 = yy + ddy, x2 = xx + ddx, z2 = zz + ddz;
-          if (y2 >= 0 && y2 < s.Y && x2 >= 0 && x2 < s.X && z2 >= 0 && z2 < s.Z)
-            ld[u] = __ldg(reinterpret_cast<const int4 *>(
-                in + ((((size_t)b * s.Y + y2) * s.X + x2) * s.Z + z2) * s.cin + ci));
+        for (int u = 0; u < 8; u++) {
+          ld[u] = make_int4(0, 0, 0, 0);
+          const int z2 = zz + u + ddz;
+          if (line && v0 + u < kend && z2 >= 0 && z2 < s.Z)
+            ld[u] = __ldg(reinterpret_cast<const int4 *>(base + (size_t)z2 * s.cin));
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          ld[u] = make_int4(0, 0, 0, 0);
+          const long long v = vb + ca * 8 + u;
+          if (ra < rows && v < kend) {
+            int b, yy, xx, zz;
+            voxel_coords(s, v, b, yy, xx, zz);
+            const int y2 = yy + ddy, x2 = xx + ddx, z2 = zz + ddz;
+            if (y2 >= 0 && y2 < s.Y && x2 >= 0 && x2 < s.X && z2 >= 0 && z2 < s.Z)
+              ld[u] = __ldg(reinterpret_cast<const int4 *>(
+                  in + ((((size_t)b * s.Y + y2) * s.X + x2) * s.Z + z2) * s.cin + ci));
+          }
         }
       }
       transpose8(ld, tr);
