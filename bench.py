@@ -352,6 +352,32 @@ def network_forward(nxy, nz, reps, weights=WEIGHTS):
     net.close()
 
 
+def network_train(nxy, nz, steps, patch, batch=8, volumes=4):
+    """`--network-train`: training steps of the warm-start network alone
+    (xtc_net_train: batches of random patches, forward, backward, Adam) on
+    `volumes` seeded random volumes [nxy][nxy][nz], after 5 untimed steps;
+    time per step and algorithmic TFLOP/s (3 x the forward's 2 x 27 x cin x
+    cout per voxel and layer)."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(0)
+    vols = [torch.rand(nxy, nxy, nz, device="cuda", generator=g) * 0.01 for _ in range(volumes)]
+    data = [(v, v * 0.9, v * 0.95) for v in vols]
+    net = xtg.WarmNet(seed=1)
+    args = ([d[0] for d in data], [d[1] for d in data], [d[2] for d in data], (nxy, nxy, nz), tuple(patch), batch)
+    net.train(*args, 5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = net.train(*args, steps)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    vox = batch * patch[0] * patch[1] * patch[2]
+    flops = 3 * sum(2.0 * 27 * ci * co * vox / 8 ** lvl for ci, co, lvl in NET_LAYERS)
+    print(json.dumps({"network_train": {"patch": list(patch), "batch": batch, "steps": steps},
+                      "ms_per_step": dt * 1e3 / steps, "tflops": flops * steps / dt / 1e12,
+                      "loss_last20": float(losses[-20:].mean())}), flush=True)
+    net.close()
+
+
 def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, coarse_iters=30, learned=True,
              weights=WEIGHTS, starts=("zero", "fbp", "multires", "learned")):
     """Seconds to MAP cost <= (1 + tol) C* from four starts:
@@ -899,7 +925,10 @@ def main():
                     help="z slices per ICD work piece (0: chosen from the L2 size)")
     ap.add_argument("--network-forward", action="store_true",
                     help="time only the warm-start network's forward pass on [1][nxy][nxy][nz] (profiling)")
-    ap.add_argument("--nz", type=int, default=64, help="slices for --network-forward")
+    ap.add_argument("--network-train", action="store_true",
+                    help="time only training steps of the warm-start network on [nxy][nxy][nz] volumes (profiling)")
+    ap.add_argument("--patch", type=int, nargs=3, default=(64, 64, 32), help="training patch for --network-train")
+    ap.add_argument("--nz", type=int, default=64, help="slices for --network-forward / --network-train")
     ap.add_argument("--reps", type=int, default=5, help="forward passes timed by --network-forward")
     ap.add_argument("--kernels", action="store_true",
                     help="time the non-ICD kernels of the engine on the workload (profiling)")
@@ -912,6 +941,8 @@ def main():
     args = ap.parse_args()
     if args.network_forward:
         network_forward(args.nxy or 512, args.nz, args.reps)
+    elif args.network_train:
+        network_train(args.nxy or 256, args.nz, args.steps, args.patch)
     elif args.kernels:
         kernel_timings(args)
     elif args.impl == "reference":
