@@ -379,7 +379,7 @@ def network_train(nxy, nz, steps, patch, batch=8, volumes=4):
 
 
 def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, coarse_iters=30, learned=True,
-             weights=WEIGHTS, starts=("zero", "fbp", "multires", "learned")):
+             weights=WEIGHTS, starts=("zero", "fbp", "multires", "learned"), cstar_start="fbp"):
     """Seconds to MAP cost <= (1 + tol) C* from four starts:
       zero     -- the reference's start, plain ICD with the benchmark's A storage;
       fbp      -- the FBP image, same A storage;
@@ -404,7 +404,10 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     import torch
     zero = np.zeros(ctx.obj_shape, np.float32)
     torch.cuda.synchronize()
-    ctx.init_fbp()
+    if cstar_start == "multires":
+        ctx.init_multires(coarse_iters)
+    else:
+        ctx.init_fbp()
     hist = []
     for it in range(1, max_iters + 1):
         ctx.iteration(it)
@@ -415,8 +418,8 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     c_star = ctx.resync_fp64()[0]
     x_star = ctx.object()
     x_scale = float(np.abs(x_star).max()) or 1.0
-    out = {"c_star": c_star, "c_star_iterations": len(hist), "tol": tol,
-           "c_star_source": "this engine from the FBP start run until its FP64 cost stalls; the MAP cost of "
+    out = {"c_star": c_star, "c_star_iterations": len(hist), "tol": tol, "c_star_start": cstar_start,
+           "c_star_source": f"this engine from the {cstar_start} start run until its FP64 cost stalls; the MAP cost of "
                             "that object is re-evaluated on the host in c_star_check (the oracle with the GPU's "
                             "arithmetic, and the reference's FP64 build's arithmetic).  With the same options "
                             "at 128^2 x 16 / 512 views the parallel schedule reaches the reference FP64 engine's "
@@ -628,7 +631,8 @@ def run_ours(args):
         # a single-GPU metric: with N replicas every rank would repeat it.
         # The committed warm-start weights were trained for the plain-3D geometry
         line["time_to_cost"] = converge(ctx, args.amode, learned=args.workload == "plain3d" and not args.nxy,
-                                        weights=args.weights, starts=tuple(args.starts.split(",")))
+                                        weights=args.weights, starts=tuple(args.starts.split(",")),
+                                        cstar_start=args.cstar_start)
         x_star = line["time_to_cost"].pop("_x_star")
         # the reference's CPU-runnable configuration, to its own FP64 converged cost
         line["time_to_cost_config1"] = config1_gpu(args.amode)
@@ -937,6 +941,8 @@ def main():
     ap.add_argument("--weights", default=WEIGHTS, help="warm-start network weights for the learned start")
     ap.add_argument("--starts", default="zero,fbp,multires,learned",
                     help="starts timed by time_to_cost (comma-separated subset)")
+    ap.add_argument("--cstar-start", default="fbp", choices=["fbp", "multires"],
+                    help="start of the run to a stall that defines C* (multires: fewer iterations on large volumes)")
     ap.add_argument("--no-converge", action="store_true", help="skip the seconds-to-converged-cost run")
     args = ap.parse_args()
     if args.network_forward:
