@@ -632,7 +632,7 @@ def run_ours(args):
         # The committed warm-start weights were trained for the plain-3D geometry
         line["time_to_cost"] = converge(ctx, args.amode, learned=args.workload == "plain3d" and not args.nxy,
                                         weights=args.weights, starts=tuple(args.starts.split(",")),
-                                        cstar_start=args.cstar_start)
+                                        cstar_start=args.cstar_start, max_iters=args.max_iters)
         x_star = line["time_to_cost"].pop("_x_star")
         # the reference's CPU-runnable configuration, to its own FP64 converged cost
         line["time_to_cost_config1"] = config1_gpu(args.amode)
@@ -815,8 +815,10 @@ def other_workload(name, args, steps=None):
         out["time_to_cost"].pop("_x_star")
         out["time_to_cost"]["learned"] = "not run: the committed network was trained for the plain-3D geometry"
     elif big:
-        out["time_to_cost"] = ("not run: its converged cost needs a run to a stall of several hundred 4.7 s "
-                               "iterations, beyond the benchmark's time")
+        out["time_to_cost"] = ("not run by default (about 30 minutes of 4-5 s iterations: a 120-iteration run "
+                               "to C* from the multi-resolution start, then each start); time it with "
+                               "`python bench.py --workload timbir4d_large --steps 1 --warmup 1 --no-cpu-baseline "
+                               "--cstar-start multires --max-iters 120`")
     ctx.close()
     return out
 
@@ -941,6 +943,8 @@ def main():
     ap.add_argument("--weights", default=WEIGHTS, help="warm-start network weights for the learned start")
     ap.add_argument("--starts", default="zero,fbp,multires,learned",
                     help="starts timed by time_to_cost (comma-separated subset)")
+    ap.add_argument("--max-iters", type=int, default=400,
+                    help="iteration limit of the run to a stall and of each timed start")
     ap.add_argument("--cstar-start", default="fbp", choices=["fbp", "multires"],
                     help="start of the run to a stall that defines C* (multires: fewer iterations on large volumes)")
     ap.add_argument("--no-converge", action="store_true", help="skip the seconds-to-converged-cost run")

@@ -12,6 +12,7 @@ Tolerances, stated per test:
   * parallel ICD: MAP cost within 1e-4 relative of the FP64 oracle's
     converged cost, and RMSE against its converged object.
 """
+import functools
 import os
 
 import numpy as np
@@ -247,7 +248,7 @@ def converged_cost_fp64(name, iters=120):
                                               ("timbir4d", xtg.XTG_A_FP16, 0), ("plain3d", xtg.XTG_A_TABLE32, 2),
                                               ("zinger_nhicd", xtg.XTG_A_TABLE32, 1), ("blocks_z", xtg.XTG_A_FP32, 4),
                                               ("launcher_geom", xtg.XTG_A_TABLE32, 0),
-                                              ("launcher_geom", xtg.XTG_A_FP16, 0)])
+                                              ("launcher_geom", xtg.XTG_A_FP16, 0), ("timbir4d", xtg.XTG_A_TABLE32, 0)])
 def test_parallel_icd_converges_to_oracle(name, amode, zslab):
     """zslab > 0 cuts every column visit into z pieces of that many slices,
     visited piece-major (the schedule large volumes use to keep e and w in L2)."""
@@ -269,6 +270,53 @@ def test_parallel_icd_converges_to_oracle(name, amode, zslab):
     # the RMSE bound is looser there.
     bound = 1e-1 if CASES[name].get("zinger") else 2e-2
     assert rmse / float(np.abs(xstar).max()) < bound
+
+
+# (parameters, oracle iterations to its converged cost)
+ITEM_CASES = {
+    # 24 detector rows, runs of ~40 entries (two frames of 20 views): 128-thread CTAs
+    "medium": (dict(N=24, NT=24, NP=40, n_time=2, nhicd=True), 120),
+    # 18 detector rows, runs of ~1100 entries (512 views): 256-thread CTAs
+    "long": (dict(N=24, NT=18, NP=512, nhicd=True), 30),
+}
+
+
+@functools.lru_cache(maxsize=None)
+def items_case(kind):
+    kw, iters = ITEM_CASES[kind]
+    p = common.params(**kw)
+    t, a = common.views(p)
+    _, _, y, w = common.data(p, t, a, seed=9)
+    o = Oracle(p, t, a, double=True)
+    o.set_sino(y, w)
+    o.init_error_sino()
+    o.srandom2(761521)
+    for it in range(1, iters + 1):
+        o.iterate(it)
+    return p, t, a, y, w, o.cost()[0], o.object()
+
+
+@pytest.mark.parametrize("kind,amode", [("medium", xtg.XTG_A_TABLE32), ("medium", xtg.XTG_A_FP16),
+                                        ("long", xtg.XTG_A_TABLE32), ("long", xtg.XTG_A_FP16)])
+def test_parallel_icd_longer_items_converge(kind, amode):
+    """Work items of more than 16 detector rows in the table modes: columns
+    whose runs hold at most 1024 entries run in 128-thread CTAs that take
+    eight items per atomic, longer ones in 256-thread CTAs; both fetch the
+    next item's table run ahead.  The parallel schedule reaches the FP64
+    oracle's converged cost within 1e-4 relative, RMSE below 2 % of the
+    object's range."""
+    p, t, a, y, w, cstar, xstar = items_case(kind)
+    c = xtg.Context(p, t, a)
+    c.set_options(a_mode=amode)
+    assert c.N_z * c.zovl > 16
+    c.upload_sino(y, w)
+    c.init_error_sino()
+    for it in range(1, 61):
+        c.iteration(it)
+    cost = c.resync_fp64()[0]
+    assert cost <= cstar * (1 + 1e-4), (cost, cstar)
+    rmse = float(np.sqrt(np.mean((c.object() - xstar) ** 2)))
+    assert rmse / float(np.abs(xstar).max()) < 2e-2
 
 
 @pytest.mark.parametrize("dxy", [1.0, 2.0])

@@ -64,6 +64,31 @@ __device__ __forceinline__ float4 ld_w(const float *p) {
   return v;
 }
 
+// Asynchronous global -> shared copies (no registers held while in flight);
+// cp_wait_all completes the calling thread's copies and makes them visible to it.
+__device__ __forceinline__ uint32_t icd_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async16(void *s, const void *g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(icd_smem(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *s, const void *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(icd_smem(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *s, const void *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(icd_smem(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Where a work item's column run lies in the A column table, fetched for the
+// next item while the current one is processed (small CTAs).
+struct ItemMeta {
+  int4 item;           // frame, row, column, z-block
+  long long s0, s1;    // tstart[ti], tstart[ti + 1]
+  float sc;            // tscale[ti] (FP16 table)
+  int rank;            // col_rank[row][column]
+  int it;              // launch-wide item index (>= the launch's total: none)
+  int pad;
+};
+
 // Footprint entries a thread loads before it uses any of them (table modes,
 // 16-byte rows): more loads in flight per warp to cover L2/HBM latency.
 #ifndef XTG_UNROLL
@@ -109,6 +134,21 @@ __device__ __forceinline__ Nbr nbr_term(const DevGeo &G, const float *sNb, const
   return o;
 }
 
+// Footprint entries each thread of a 64-thread CTA keeps in flight through
+// asynchronous copies into shared memory (table modes, parallel schedule,
+// 16-byte rows); 0 = loads into registers like the larger CTAs.
+// Next-item prefetch in the 256-thread CTAs too (the small ones always)
+#ifndef XTG_PF_ALL
+#define XTG_PF_ALL 0
+#endif
+#ifndef XTG_SMALL_RING
+#define XTG_SMALL_RING 0
+#endif
+template <int VEC, int AMODE, int SEQ, int NT>
+__host__ __device__ constexpr int icd_ring() {
+  return (NT == XTG_SMALL_NT && VEC == 4 && AMODE != 0 && !SEQ) ? XTG_SMALL_RING : 0;
+}
+
 // NT threads per CTA: 256 for long z-lines; 64 where a work item is short
 // (few detector rows), so the per-item fixed work (neighbourhood, A staging,
 // barriers, the surrogate step) runs in four times as many CTAs at once.
@@ -116,15 +156,21 @@ template <int VEC, int AMODE, int SEQ, int AS, int NT = XTG_THREADS>
 __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_columns(DevGeo G, IcdArgs A, int vmax,
                                                                                  int zmax) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NW = NT / 32;
+  // (64-thread CTAs) each thread's ring of RING footprint entries in flight,
+  // {e row, w row} of 16 bytes each, filled by asynchronous copies
+  constexpr int RING = icd_ring<VEC, AMODE, SEQ, NT>();
+  float4 *sRing = reinterpret_cast<float4 *>(smem_raw);  // [NT][RING][2]
+  unsigned char *smem = smem_raw + (size_t)NT * RING * 32;
   // AMODE 0 (A computed here): per view {first | n << 24, view index, AS values}
-  int *sPack = reinterpret_cast<int *>(smem_raw);        // [vmax]
+  int *sPack = reinterpret_cast<int *>(smem);            // [vmax]
   int *sView = sPack + vmax;                              // [vmax]
   float *sVal = reinterpret_cast<float *>(sView + vmax);  // [AS][vmax] A * delta_t
   // AMODE 1/2 (column table): the column's entry run, vmax = longest run,
   // {(p*N_r + bin)*N_t, bits of A * delta_t} per entry (one 8-byte load)
-  int2 *sEnt = reinterpret_cast<int2 *>(smem_raw);       // [vmax]
-  float *sRed = (AMODE == 0) ? sVal + (size_t)vmax * AS : reinterpret_cast<float *>(sEnt + vmax);  // [2][8][128]
-  float *sTh = sRed + 2 * 8 * 128;                        // [2][zmax*zovl]
+  int2 *sEnt = reinterpret_cast<int2 *>(smem);           // [vmax]
+  float *sRed = (AMODE == 0) ? sVal + (size_t)vmax * AS : reinterpret_cast<float *>(sEnt + vmax);  // [2][NW][128]
+  float *sTh = sRed + 2 * NW * 128;                       // [2][zmax*zovl]
   const int rowsmax = zmax * G.zovl;
   float *sNb = sTh + 2 * rowsmax;                         // [9][zmax+2]
   float *sTn = sNb + 9 * (zmax + 2);                      // [2][zmax]
@@ -146,29 +192,77 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
   __shared__ int sGrab[2];                 // base, next of the batch
   __shared__ double sCtaAbs;
   __shared__ unsigned long long sCta[3];   // voxel updates, zero skipped, items
+  // Small CTAs fetch the next item's record and table run asynchronously in
+  // three dependent steps (record; column rank; run bounds), one per phase of
+  // the current item, so that the chain's round trips overlap its work.
+  constexpr bool PF = (NT < XTG_THREADS || XTG_PF_ALL) && AMODE != 0 && !SEQ;
+  __shared__ __align__(16) ItemMeta sMeta[2];
+  int mb = 0;  // sMeta[mb]: the current item; sMeta[mb ^ 1]: the next
+  const int total = nitems * A.nsub;
+  auto grab = [&]() -> int {  // thread 0 only
+    if (sGrab[1] == GRAB) {
+      sGrab[0] = atomicAdd(A.counter, GRAB);
+      sGrab[1] = 0;
+    }
+    return sGrab[0] + sGrab[1]++;
+  };
+  auto item_index = [&](int i) -> int {
+    const int ii = i % nitems;
+    return A.item_lo + (A.use_perm ? (int)xt_perm((uint32_t)ii, (uint32_t)nitems, A.perm_key) : ii);
+  };
+  // the rank and run-bound steps with plain loads (prologue, skipped pieces)
+  auto fetch_rank = [&]() {  // thread 0, the next item's record in place
+    ItemMeta &N = sMeta[mb ^ 1];
+    if (N.it < total) cp_async4(&N.rank, A.col_rank + N.item.y * G.N_x + N.item.z);
+  };
+  auto fetch_bounds = [&]() {  // thread 0, the next item's rank in place
+    ItemMeta &N = sMeta[mb ^ 1];
+    if (N.it < total) {
+      const long long ti = (long long)N.item.x * A.n_masked + N.rank;
+      cp_async8(&N.s0, A.tstart + ti);
+      cp_async8(&N.s1, A.tstart + ti + 1);
+      if (AMODE == 1) cp_async4(&N.sc, A.tscale + ti);
+    }
+  };
+  auto meta_finish = [&](ItemMeta &N) {
+    if (N.it >= total) return;
+    N.rank = A.col_rank[N.item.y * G.N_x + N.item.z];
+    const long long ti = (long long)N.item.x * A.n_masked + N.rank;
+    N.s0 = A.tstart[ti];
+    N.s1 = A.tstart[ti + 1];
+    N.sc = (AMODE == 1) ? A.tscale[ti] : 1.f;
+  };
   if (tid == 0) {
     sGrab[0] = 0;
     sGrab[1] = GRAB;
     sCtaAbs = 0.0;
     sCta[0] = sCta[1] = sCta[2] = 0;
+    if (PF) {
+      sMeta[0].it = grab();
+      if (sMeta[0].it < total) {
+        sMeta[0].item = A.items[item_index(sMeta[0].it)];
+        meta_finish(sMeta[0]);
+      }
+    }
   }
 
   for (;;) {
     if (tid == 0) {
-      if (sGrab[1] == GRAB) {
-        sGrab[0] = atomicAdd(A.counter, GRAB);
-        sGrab[1] = 0;
+      if (PF) {
+        ItemMeta &N = sMeta[mb ^ 1];
+        N.it = grab();
+        if (N.it < total) cp_async16(&N.item, A.items + item_index(N.it));
+      } else {
+        sItem = grab();
       }
-      sItem = sGrab[0] + sGrab[1]++;
       sUpd = 0;
       sZero = 0;
     }
     __syncthreads();
-    const int it = sItem;
-    if (it >= nitems * A.nsub) break;
-    const int piece = it / nitems, ii = it - piece * nitems;
-    const int q = A.use_perm ? (int)xt_perm((uint32_t)ii, (uint32_t)nitems, A.perm_key) : ii;
-    const int4 item = A.items[A.item_lo + q];
+    const int it = PF ? sMeta[mb].it : sItem;
+    if (it >= total) break;
+    const int piece = it / nitems;
+    const int4 item = PF ? sMeta[mb].item : A.items[item_index(it)];
     const int fr = item.x, row = item.y, col = item.z, blk = item.w;
     int zb = 0, ze = G.N_z - 1;
     if (blk >= 0) {
@@ -177,7 +271,12 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     }
     zb += piece * A.zslab;
     if (zb > ze) {  // this item has fewer pieces (uniform over the CTA)
+      if (PF && tid == 0) {
+        cp_wait_all();
+        meta_finish(sMeta[mb ^ 1]);
+      }
       __syncthreads();
+      mb ^= 1;
       continue;
     }
     ze = min(ze, zb + A.zslab - 1);
@@ -190,6 +289,18 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     //    as the reference's ranks read Object[i][0] / [N_z+1],
     //    XT_VoxUpdate.c:94-99)
     const size_t plane = (size_t)G.N_y * G.N_x;
+    // (small CTAs, FP32 table) the column's table run goes to shared memory
+    // asynchronously first, so that its round trip overlaps the
+    // neighbourhood's; a quiet line (below) has fetched it for nothing
+    constexpr bool PFE = PF && AMODE == 2;
+    if (PFE) {
+      const long long s0 = sMeta[mb].s0;
+      const int n = (int)(sMeta[mb].s1 - s0);
+      for (int e = tid; e < n; e += NT) {
+        cp_async4(&sEnt[e].x, A.toff + s0 + e);
+        cp_async4(&sEnt[e].y, A.tval32 + s0 + e);
+      }
+    }
     for (int k = tid; k < 9 * (Z + 2); k += NT) {
       const int c = k / (Z + 2), zz = k - c * (Z + 2);
       const int jj = row + c / 3 - 1, kk = col + c % 3 - 1, za = zb - 1 + zz;
@@ -245,16 +356,36 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     }
     int ne = 0;
     if (AMODE != 0 && !skip_all) {
-      const long long ti = (long long)fr * A.n_masked + A.col_rank[row * G.N_x + col];
-      const long long s0 = A.tstart[ti];
-      ne = (int)(A.tstart[ti + 1] - s0);
-      const float sc = (AMODE == 1) ? A.tscale[ti] : 1.f;
-      for (int e = tid; e < ne; e += NT) {
-        const float a = (AMODE == 2) ? __ldg(A.tval32 + s0 + e) : __half2float(A.tval16[s0 + e]) * sc;
-        sEnt[e] = make_int2(__ldg(A.toff + s0 + e), __float_as_int(a));
+      long long s0;
+      float sc;
+      if (PF) {
+        s0 = sMeta[mb].s0;
+        ne = (int)(sMeta[mb].s1 - s0);
+        sc = sMeta[mb].sc;
+      } else {
+        const long long ti = (long long)fr * A.n_masked + A.col_rank[row * G.N_x + col];
+        s0 = A.tstart[ti];
+        ne = (int)(A.tstart[ti + 1] - s0);
+        sc = (AMODE == 1) ? A.tscale[ti] : 1.f;
+      }
+      if (!PFE) {
+        for (int e = tid; e < ne; e += NT) {
+          const float a = (AMODE == 2) ? __ldg(A.tval32 + s0 + e) : __half2float(A.tval16[s0 + e]) * sc;
+          sEnt[e] = make_int2(__ldg(A.toff + s0 + e), __float_as_int(a));
+        }
       }
     }
+    if (PFE) cp_wait_all();
     __syncthreads();
+    // The next item's chain steps are issued by thread 0 where a phase of
+    // this item follows that needs none of its own asynchronous copies (its
+    // waits complete every copy it has in flight): the rank during the
+    // footprint loop (bounds after it) with register loads, after it with
+    // the ring.
+    if (PF && tid == 0) {
+      cp_wait_all();  // the next item's record
+      if (RING == 0) fetch_rank();
+    }
 
     // 3. theta1 / theta2 over the column's footprint (XT_VoxUpdate.c:20-51)
     const int tln = (T + VEC - 1) / VEC;
@@ -340,6 +471,37 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
           for (int s = 0; s < AS; s++)
             if (s < n) accumulate(off + s * G.N_t, sVal[s * vmax + v]);
         }
+      } else if (RING > 0) {
+        // entries vg, vg + vgs, ...: RING of them in flight in this thread's
+        // ring (one commit group per entry, empty past the end), each slot
+        // refilled after its values have been used
+        constexpr int RSZ = RING > 0 ? RING : 1;
+        float4 *ring = sRing + (size_t)tid * RING * 2;
+        const int m = (ne - vg + vgs - 1) / vgs;
+        uint64_t pe, pw;
+        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pe));
+        asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pw));
+        auto fill = [&](int k) {
+          if (k < m) {
+            const int off = sEnt[vg + k * vgs].x;
+            float4 *r = ring + (k % RSZ) * 2;
+            asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(icd_smem(r)),
+                         "l"(eb + off), "l"(pe)
+                         : "memory");
+            asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(icd_smem(r + 1)),
+                         "l"(wb + off), "l"(pw)
+                         : "memory");
+          }
+          asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+#pragma unroll
+        for (int k = 0; k < RSZ; k++) fill(k);
+        for (int k = 0; k < m; k++) {
+          asm volatile("cp.async.wait_group %0;" ::"n"(RSZ - 1) : "memory");
+          const float4 *r = ring + (k % RSZ) * 2;
+          accumulate_vals(r[0], r[1], __int_as_float(sEnt[vg + k * vgs].y));
+          fill(k + RSZ);
+        }
       } else if (VEC == 4) {
         int e = vg;
         for (; e + (XTG_UNROLL - 1) * vgs < ne; e += XTG_UNROLL * vgs) {
@@ -378,16 +540,23 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
 #pragma unroll
       for (int c = 0; c < VEC; c++) {
         sRed[warp * 128 + tl * VEC + c] = th1[c];
-        sRed[8 * 128 + warp * 128 + tl * VEC + c] = th2[c];
+        sRed[NW * 128 + warp * 128 + tl * VEC + c] = th2[c];
       }
     }
     __syncthreads();
+    if (PF && tid == 0) {
+      cp_wait_all();
+      if (RING == 0)
+        fetch_bounds();
+      else
+        fetch_rank();
+    }
     for (int t = tid; t < T; t += NT) {
       float s1 = 0.f, s2 = 0.f;
 #pragma unroll
-      for (int wq = 0; wq < NT / 32; wq++) {  // every warp wrote its partial (zeros if idle)
+      for (int wq = 0; wq < NW; wq++) {  // every warp wrote its partial (zeros if idle)
         s1 += sRed[wq * 128 + t];
-        s2 += sRed[8 * 128 + wq * 128 + t];
+        s2 += sRed[NW * 128 + wq * 128 + t];
       }
       sTh[t] = s1;
       sTh[rowsmax + t] = s2;
@@ -510,6 +679,10 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
       }
     }
     __syncthreads();
+    if (PF && RING > 0 && tid == 0) {
+      cp_wait_all();
+      fetch_bounds();
+    }
 
     // 5. MagUpdateMap[frame][block][row][col] = sum |delta| over the block's
     //    slices of this visit (XT_VoxUpdate.c:128, 236); sum |x| and counters
@@ -579,7 +752,9 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
         }
       }
     }
+    if (PF && tid == 0) cp_wait_all();  // the next item's meta is complete
     __syncthreads();
+    mb ^= 1;
   }
   if (tid == 0 && (sCta[0] || sCta[1] || sCta[2] || sCtaAbs != 0.0)) {  // pieces past the first count no item
     atomicAdd(&A.st_absx[blockIdx.x & 63], sCtaAbs);
@@ -589,13 +764,14 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
   }
 }
 
-size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec) {
+size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec, int nt) {
   size_t b = 0;
+  if (nt == XTG_SMALL_NT && vec == 4 && amode != 0) b += (size_t)nt * XTG_SMALL_RING * 32;  // sRing
   if (amode == 0)
     b += (size_t)vmax * (4 * 2 + 4 * (size_t)as);  // sPack, sView, sVal
   else
     b += (size_t)vmax * 8;                         // sEnt
-  b += 2 * 8 * 128 * 4;                            // sRed
+  b += 2 * (size_t)(nt / 32) * 128 * 4;            // sRed
   b += 2 * (size_t)zmax * zovl * 4;                // sTh
   b += 9 * (size_t)(zmax + 2) * 4;                 // sNb
   b += 2 * (size_t)zmax * 4;                       // sTn
@@ -655,8 +831,8 @@ int icd_threads(int vec, int amode, int seq, int zmax, int zovl, int vmax) {
 
 cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, int seq, int as, int vmax, int zmax,
                        int grid, cudaStream_t st) {
-  const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as, amode, vec);
   const int nt = icd_threads(vec, amode, seq, zmax, G.zovl, vmax);
+  const size_t smem = icd_smem_bytes(vmax, zmax, G.zovl, as, amode, vec, nt);
   IcdKernel k = icd_kernel(vec, amode, seq, as, nt);
   cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -670,8 +846,8 @@ cudaError_t launch_icd(const DevGeo &G, const IcdArgs &A, int vec, int amode, in
 }
 
 int icd_occupancy(int vec, int amode, int seq, int as, int vmax, int zmax, int zovl) {
-  const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as, amode, vec);
   const int nt = icd_threads(vec, amode, seq, zmax, zovl, vmax);
+  const size_t smem = icd_smem_bytes(vmax, zmax, zovl, as, amode, vec, nt);
   IcdKernel k = icd_kernel(vec, amode, seq, as, nt);
   int nb = 0;
   cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -83,7 +83,7 @@ cudaError_t launch_fp_csr(const DevGeo &G, const FpArgs &F, const CsrView &T, in
 cudaError_t launch_table_count(const DevGeo &G, const TableArgs &T, int ns, long long *count, cudaStream_t st);
 cudaError_t launch_table_fill(const DevGeo &G, const TableArgs &T, int ns, cudaStream_t st);
 
-size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec);
+size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec, int nt);
 cudaError_t launch_fbp(const DevGeo &G, const float *y, const float *d, float *q, const float *cosv,
                        const float *sinv, const int *view_idx, const int *view_start, const int *view_num,
                        const int *col_rank, float *x, cudaStream_t st);
