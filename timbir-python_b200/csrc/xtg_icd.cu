@@ -134,20 +134,12 @@ __device__ __forceinline__ Nbr nbr_term(const DevGeo &G, const float *sNb, const
   return o;
 }
 
-// Footprint entries each thread of a 64-thread CTA keeps in flight through
-// asynchronous copies into shared memory (table modes, parallel schedule,
-// 16-byte rows); 0 = loads into registers like the larger CTAs.
-// Next-item prefetch in the 256-thread CTAs too (the small ones always)
+// Next-item prefetch in the 256-thread CTAs too (the small ones always):
+// measured equal on plain 3D (237.6-238.5 against 236.5-237.1 M voxel
+// updates/s), so off
 #ifndef XTG_PF_ALL
 #define XTG_PF_ALL 0
 #endif
-#ifndef XTG_SMALL_RING
-#define XTG_SMALL_RING 0
-#endif
-template <int VEC, int AMODE, int SEQ, int NT>
-__host__ __device__ constexpr int icd_ring() {
-  return (NT == XTG_SMALL_NT && VEC == 4 && AMODE != 0 && !SEQ) ? XTG_SMALL_RING : 0;
-}
 
 // NT threads per CTA: 256 for long z-lines; 64 where a work item is short
 // (few detector rows), so the per-item fixed work (neighbourhood, A staging,
@@ -157,11 +149,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
                                                                                  int zmax) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NW = NT / 32;
-  // (64-thread CTAs) each thread's ring of RING footprint entries in flight,
-  // {e row, w row} of 16 bytes each, filled by asynchronous copies
-  constexpr int RING = icd_ring<VEC, AMODE, SEQ, NT>();
-  float4 *sRing = reinterpret_cast<float4 *>(smem_raw);  // [NT][RING][2]
-  unsigned char *smem = smem_raw + (size_t)NT * RING * 32;
+  unsigned char *smem = smem_raw;
   // AMODE 0 (A computed here): per view {first | n << 24, view index, AS values}
   int *sPack = reinterpret_cast<int *>(smem);            // [vmax]
   int *sView = sPack + vmax;                              // [vmax]
@@ -380,11 +368,10 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     // The next item's chain steps are issued by thread 0 where a phase of
     // this item follows that needs none of its own asynchronous copies (its
     // waits complete every copy it has in flight): the rank during the
-    // footprint loop (bounds after it) with register loads, after it with
-    // the ring.
+    // footprint loop, the run bounds during the surrogate step.
     if (PF && tid == 0) {
       cp_wait_all();  // the next item's record
-      if (RING == 0) fetch_rank();
+      fetch_rank();
     }
 
     // 3. theta1 / theta2 over the column's footprint (XT_VoxUpdate.c:20-51)
@@ -471,37 +458,6 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
           for (int s = 0; s < AS; s++)
             if (s < n) accumulate(off + s * G.N_t, sVal[s * vmax + v]);
         }
-      } else if (RING > 0) {
-        // entries vg, vg + vgs, ...: RING of them in flight in this thread's
-        // ring (one commit group per entry, empty past the end), each slot
-        // refilled after its values have been used
-        constexpr int RSZ = RING > 0 ? RING : 1;
-        float4 *ring = sRing + (size_t)tid * RING * 2;
-        const int m = (ne - vg + vgs - 1) / vgs;
-        uint64_t pe, pw;
-        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pe));
-        asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pw));
-        auto fill = [&](int k) {
-          if (k < m) {
-            const int off = sEnt[vg + k * vgs].x;
-            float4 *r = ring + (k % RSZ) * 2;
-            asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(icd_smem(r)),
-                         "l"(eb + off), "l"(pe)
-                         : "memory");
-            asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(icd_smem(r + 1)),
-                         "l"(wb + off), "l"(pw)
-                         : "memory");
-          }
-          asm volatile("cp.async.commit_group;" ::: "memory");
-        };
-#pragma unroll
-        for (int k = 0; k < RSZ; k++) fill(k);
-        for (int k = 0; k < m; k++) {
-          asm volatile("cp.async.wait_group %0;" ::"n"(RSZ - 1) : "memory");
-          const float4 *r = ring + (k % RSZ) * 2;
-          accumulate_vals(r[0], r[1], __int_as_float(sEnt[vg + k * vgs].y));
-          fill(k + RSZ);
-        }
       } else if (VEC == 4) {
         int e = vg;
         for (; e + (XTG_UNROLL - 1) * vgs < ne; e += XTG_UNROLL * vgs) {
@@ -546,10 +502,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     __syncthreads();
     if (PF && tid == 0) {
       cp_wait_all();
-      if (RING == 0)
-        fetch_bounds();
-      else
-        fetch_rank();
+      fetch_bounds();
     }
     for (int t = tid; t < T; t += NT) {
       float s1 = 0.f, s2 = 0.f;
@@ -679,10 +632,6 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
       }
     }
     __syncthreads();
-    if (PF && RING > 0 && tid == 0) {
-      cp_wait_all();
-      fetch_bounds();
-    }
 
     // 5. MagUpdateMap[frame][block][row][col] = sum |delta| over the block's
     //    slices of this visit (XT_VoxUpdate.c:128, 236); sum |x| and counters
@@ -766,7 +715,6 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
 
 size_t icd_smem_bytes(int vmax, int zmax, int zovl, int as, int amode, int vec, int nt) {
   size_t b = 0;
-  if (nt == XTG_SMALL_NT && vec == 4 && amode != 0) b += (size_t)nt * XTG_SMALL_RING * 32;  // sRing
   if (amode == 0)
     b += (size_t)vmax * (4 * 2 + 4 * (size_t)as);  // sPack, sView, sVal
   else
