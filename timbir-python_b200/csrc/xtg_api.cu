@@ -54,6 +54,14 @@ void xtg_set_error_text(const char *msg) { snprintf(g_err, sizeof g_err, "%s", m
 #define NSLOT 64
 // parallel ICD: at most 1 in XTG_CONC_DIV of the columns updated at once
 #define XTG_CONC_DIV 32
+// ICD footprint loads keep w in L2 (like e) when e and w together take at
+// most XTG_W_KEEP_BYTES; larger sinograms evict w first
+#ifndef XTG_W_KEEP
+#define XTG_W_KEEP 1
+#endif
+#ifndef XTG_W_KEEP_BYTES
+#define XTG_W_KEEP_BYTES (48u << 20)
+#endif
 
 struct RsState;  // radix-select state per segment (defined with its kernels)
 
@@ -1743,6 +1751,7 @@ static int run_columns(xtg_ctx *c, int iter, const int4 *items, int lo, int n, c
   A.T2 = g.T * g.T; A.Tdelta = g.T * g.delta; A.st_absx = c->d_absx; A.st_cnt = c->d_cnt; A.err = c->d_err;
   A.zslab = hz; A.nsub = nsub;
   A.halo_lo = c->halo_lo; A.halo_hi = c->halo_hi;
+  A.w_keep = XTG_W_KEEP && 2 * c->ns * 4 <= (size_t)XTG_W_KEEP_BYTES;
   if (nsub > 1) {
     CK(launch_magmap_zero(c->G, A, c->sm_count * 4, c->st));
     c->launches++;

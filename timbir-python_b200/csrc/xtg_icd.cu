@@ -54,9 +54,12 @@ __device__ __forceinline__ float4 ld_e(const float *p) {
                : "l"(p), "l"(pol));
   return v;
 }
-__device__ __forceinline__ float4 ld_w(const float *p) {
+__device__ __forceinline__ float4 ld_w(const float *p, bool keep) {
   uint64_t pol;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  if (keep)  // e and w fit in L2 together: keep w as well
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  else
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
   float4 v;
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
       : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
       float ev[VEC], wv[VEC];
       if (VEC == 4) {
         const float4 e4 = ld_e(eb + off);
-        const float4 w4 = ld_w(wb + off);
+        const float4 w4 = ld_w(wb + off, A.w_keep);
         ev[0] = e4.x; ev[1] = e4.y; ev[2] = e4.z; ev[3] = e4.w;
         wv[0] = w4.x; wv[1] = w4.y; wv[2] = w4.z; wv[3] = w4.w;
       } else {
@@ -468,7 +471,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
 #pragma unroll
           for (int u = 0; u < XTG_UNROLL; u++) {
             e4[u] = ld_e(eb + en[u].x);
-            w4[u] = ld_w(wb + en[u].x);
+            w4[u] = ld_w(wb + en[u].x, A.w_keep);
           }
 #pragma unroll
           for (int u = 0; u < XTG_UNROLL; u++) accumulate_vals(e4[u], w4[u], __int_as_float(en[u].y));

@@ -31,6 +31,7 @@ struct IcdArgs {
   const float *tscale;      // per (frame, column) scale of the FP16 table
   const int *col_rank;      // [N_y*N_x] -> rank in the masked list, -1 outside
   int n_masked;
+  int w_keep;  // e and w fit in L2 together: w loads keep their lines (evict_last)
   int iter;
   float T2, Tdelta;
   // z slab of a larger volume: the neighbouring slabs' boundary slices,
