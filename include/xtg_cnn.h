@@ -41,6 +41,14 @@ int xtc_conv3d_path(const void *in, const void *w, const float *bias, void *out,
 int xtc_conv3d_wgrad(const void *in, const void *dout, float *dw, int32_t nb, int32_t Y, int32_t X, int32_t Z,
                      int32_t cin, int32_t cout);
 
+/* xtc_conv3d_wgrad with the kernel chosen: XTC_CONV_AUTO (what xtc_conv3d_wgrad does), XTC_CONV_GATHER
+ * (operands gathered and transposed per K stage by the CTA's threads) or XTC_CONV_TILE (dout and the input
+ * halo staged by TMA per tile of 128 x 2 voxels, the three dy taps stacked along M and the three dz taps
+ * along N of each MMA; cout 32, cin a multiple of 16, X a multiple of 128, Z even, else XTG_E_ARG).  AUTO
+ * uses the tile kernel wherever it applies. */
+int xtc_conv3d_wgrad_path(const void *in, const void *dout, float *dw, int32_t nb, int32_t Y, int32_t X, int32_t Z,
+                          int32_t cin, int32_t cout, int32_t path);
+
 /* ---- the warm-start network ------------------------------------------------
  * A 3D encoder-decoder over channels-last volumes: four levels with 32, 48,
  * 64 and 96 channels, two 3x3x3 convolutions + ReLU per level on each side,

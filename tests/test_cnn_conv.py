@@ -132,6 +132,38 @@ def test_conv_weight_gradient(shape):
     assert torch.max(torch.abs(got - ref_rows)) <= 1e-4 * torch.max(torch.abs(ref_rows))
 
 
+WGRAD_TILE_SHAPES = [  # nb, Y, X, Z, cin, cout: 1-5 input chunks (one or two chunk groups), batches, y edges
+    (1, 3, 128, 4, 32, 32),
+    (2, 2, 128, 6, 48, 32),
+    (1, 3, 256, 2, 80, 32),
+    (1, 1, 128, 2, 16, 32),
+]
+
+
+@pytest.mark.parametrize("shape", WGRAD_TILE_SHAPES)
+def test_tile_weight_gradient(shape):
+    """The TMA tile weight gradient (dy taps stacked along M, dz taps along
+    N) against PyTorch, and the gather kernel on the same data."""
+    lib = xtg.gpu_lib()
+    nb, Y, X, Z, cin, cout = shape
+    x, w, b = case(shape, 4)
+    g = torch.Generator().manual_seed(11)
+    dy = torch.randn(nb, cout, Y, X, Z, generator=g).to(torch.bfloat16).float()
+    ref = torch.nn.grad.conv3d_weight(x, w.shape, dy, padding=1)
+    ref_rows = ref.permute(2, 3, 4, 1, 0).reshape(27 * cin, cout)
+    xd = to_cl(x).to(torch.bfloat16).cuda()
+    dyd = to_cl(dy).to(torch.bfloat16).cuda()
+    got = {}
+    for path in (TILE, GATHER, AUTO):
+        dw = torch.zeros(27 * cin, cout, dtype=torch.float32, device="cuda")
+        check(lib.xtc_conv3d_wgrad_path(ptr(xd), ptr(dyd), ptr(dw), nb, Y, X, Z, cin, cout, path))
+        got[path] = dw.cpu()
+    tol = 1e-4 * torch.max(torch.abs(ref_rows))
+    assert torch.max(torch.abs(got[TILE] - ref_rows)) <= tol
+    assert torch.max(torch.abs(got[GATHER] - ref_rows)) <= tol
+    assert torch.max(torch.abs(got[AUTO] - got[TILE])) <= tol  # the automatic choice is the tile kernel
+
+
 def conv_path(lib, xd, wd, bd, out, shape, epi, sign, path):
     nb, Y, X, Z, cin, cout = shape
     return lib.xtc_conv3d_path(ptr(xd), ptr(wd), ptr(bd) if bd is not None else None, ptr(out), nb, Y, X, Z, cin,

@@ -103,14 +103,23 @@ int xtc_conv3d(const void *in, const void *w, const float *bias, void *out, int3
 
 int xtc_conv3d_wgrad(const void *in, const void *dout, float *dw, int32_t nb, int32_t Y, int32_t X, int32_t Z,
                      int32_t cin, int32_t cout) {
-  if (!in || !dout || !dw) {
+  return xtc_conv3d_wgrad_path(in, dout, dw, nb, Y, X, Z, cin, cout, XTC_CONV_AUTO);
+}
+
+int xtc_conv3d_wgrad_path(const void *in, const void *dout, float *dw, int32_t nb, int32_t Y, int32_t X, int32_t Z,
+                          int32_t cin, int32_t cout, int32_t path) {
+  if (!in || !dout || !dw || path < XTC_CONV_AUTO || path > XTC_CONV_TILE) {
     xtg_set_error_text("xtc_conv3d_wgrad: bad argument");
     return XTG_E_ARG;
   }
   int rc = ensure_err();
   if (rc) return rc;
   xtc::ConvShape s{nb, Y, X, Z, cin, cout, 0};
-  cudaError_t e = xtc::conv_wgrad(s, (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)dout, dw, g_err, 0);
+  if (path == XTC_CONV_TILE && !xtc::wgrad_tile_supported(s)) {
+    xtg_set_error_text("xtc_conv3d_wgrad: shape not supported by the tile kernel");
+    return XTG_E_ARG;
+  }
+  cudaError_t e = xtc::conv_wgrad(s, (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)dout, dw, g_err, 0, path);
   if (e != cudaSuccess) return fail(e, "xtc_conv3d_wgrad");
   e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) return fail(e, "xtc_conv3d_wgrad");

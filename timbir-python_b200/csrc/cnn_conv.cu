@@ -452,8 +452,14 @@ cudaError_t conv_forward(const ConvShape &s, const __nv_bfloat16 *in, const __nv
 }
 
 cudaError_t conv_wgrad(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, float *dw, int *err,
-                       cudaStream_t st) {
+                       cudaStream_t st, int path) {
   if (s.n % 16 || s.n < 16 || s.n > 256 || s.cin % 8) return cudaErrorInvalidValue;
+  if (path != 1 && wgrad_tile_supported(s)) {
+    const cudaError_t e = conv_wgrad_tile(s, in, dout, dw, err, st);
+    if (e != cudaErrorNotSupported || path == 2) return e;
+  } else if (path == 2) {
+    return cudaErrorNotSupported;
+  }
   const long long M = (long long)s.nb * s.Y * s.X * s.Z;
   const int mt = (27 * s.cin + 127) / 128;
   // enough K splits to fill the GPU twice over, each a multiple of KT voxels

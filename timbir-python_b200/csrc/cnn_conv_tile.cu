@@ -279,6 +279,192 @@ __global__ void k_pack_tile_w(int cin, int n, int kpad, int sign, const __nv_bfl
   }
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradient on staged tiles (cout = 32, cin a multiple of 16, X a
+// multiple of 128, Z even):
+//   dW[dy, dx, dz][ci][co] = sum_v dY[v][co] X[v + (dy, dx, dz)][ci]
+//                          = sum_u dY[u - (dy, 0, 0)][co] X[u + (0, dx, dz)][ci]
+// (dY and X are zero outside the volume, so the substitution v = u - dy
+// drops nothing).  In the second form one MMA covers the three dy taps along
+// M and the three dz taps along N.  A CTA walks tiles u = 128 x-voxels x 2
+// z-lines of one y-row y0 and keeps D[(dy, co)][(dx, dz, ci)] for up to three
+// 16-channel input chunks in TMEM over all its tiles.  Per tile it stages, by
+// TMA, one 32-byte row (16 channels) per voxel:
+//   A (M x K, MN-major): dY rows y0 + 1, y0, y0 - 1 (dy = -1, 0, +1) x 2
+//     channel halves = 6 boxes of 2 x 128 rows, stacked along M at a uniform
+//     atom stride (M = 96; the MMA's rows 96..127 read the next box and are
+//     discarded);
+//   B (N x K, MN-major): per input chunk, the X halo of row y0
+//     (130 x-voxels x 4 z-lines, zero fill outside); for (dx, output line z)
+//     the three z-lines z - 1, z, z + 1 (dz = -1, 0, +1) are atoms one z-line
+//     (130 rows) apart, and dx shifts the start row.
+// K is the x-voxel: 16 rows per MMA.  Warp 4 (one thread) issues the copies
+// and MMAs through two stages; warps 0-2 (TMEM lanes = (dy, co)) add the
+// accumulators into dw once at the end.  Every wait is bounded.
+constexpr int WG_TZ = 2;                                 // output z-lines per tile
+constexpr uint32_t WG_XB = (WG_TZ + 2) * TXS * 32;       // one X box: 16,640 bytes
+constexpr uint32_t WG_XS = (WG_XB + 1023) / 1024 * 1024; // its stride in a stage
+constexpr uint32_t WG_DB = WG_TZ * TX * 32;              // one dY box: 8,192 bytes
+constexpr uint32_t WG_A = 6 * WG_DB;                     // 3 y-rows x 2 channel halves
+constexpr int WG_CPG = 3;                                // input chunks per CTA: 3 x 144 TMEM columns
+constexpr uint32_t WG_SLACK = 16384;                     // past the second stage
+constexpr int WG_N = 48;                                 // 3 dz x 16 channels
+
+__host__ __device__ constexpr uint32_t wg_stage(int cpg) { return WG_A + (uint32_t)cpg * WG_XS; }
+
+// MN-major operand, 32-byte swizzle: 16-element (32-byte) rows, one per K
+// index, 8-row groups 256 bytes apart (SBO); MN atoms of 16 elements `lbo`
+// bytes apart (LBO).
+__device__ __forceinline__ uint64_t sdesc_mn_sw32(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)(256 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)6 << 61);
+}
+
+__global__ void __launch_bounds__(160, 1)
+    k_wgrad_tile(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tdy, ConvShape s,
+                 float *dw, int slices, int *err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ uint64_t full[2], empty[2], acc_full;
+  __shared__ uint32_t tbase;
+  __shared__ volatile int bad;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nchunk = s.cin >> 4;
+  const int cpg = nchunk < WG_CPG ? nchunk : WG_CPG;
+  const uint32_t STAGE = wg_stage(cpg);
+  const int grp = (int)blockIdx.x / slices, slice = (int)blockIdx.x % slices;
+  const int c0 = grp * cpg, nck = nchunk - c0 < cpg ? nchunk - c0 : cpg;
+  const int XT = s.X / TX, ZT = s.Z / WG_TZ;
+  const int ntiles = XT * ZT * s.nb * s.Y;
+  const int mine = ntiles > slice ? (ntiles - 1 - slice) / slices + 1 : 0;
+  const long long lim = 1ll << 24;
+  if (tid == 0) {
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(&acc_full, 1);
+    mbar_init_fence();
+    bad = 0;
+  }
+  if (warp == 0) tmem_alloc(&tbase, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tbase;
+  const int ncols = nck * 3 * WG_N;
+  if (warp < 4) {
+    for (int col = 0; col < ncols; col += 16) tmem_st16_zero(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col);
+    tmem_st_wait();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  auto tile_of = [&](int tl, int &x0, int &z0, int &y, int &b) {
+    int t = slice + tl * slices;
+    x0 = (t % XT) * TX;
+    t /= XT;
+    z0 = (t % ZT) * WG_TZ;
+    t /= ZT;
+    y = t % s.Y;
+    b = t / s.Y;
+  };
+  if (warp == 4) {
+    if (lane == 0) {
+      bool ok = true;
+      if (mine > 0) {
+        const uint32_t idesc = idesc_bf16(WG_N, 1, 1);
+        int issued[2] = {0, 0}, landed[2] = {0, 0};
+        auto load = [&](int q) {
+          const int st = q & 1;
+          int x0, z0, y, b;
+          tile_of(q, x0, z0, y, b);
+          uint8_t *g = sm + st * STAGE;
+          mbar_expect_tx(&full[st], 6 * WG_DB + (uint32_t)nck * WG_XB);
+          // box j = dy + 1 holds dY row y0 - dy (zero fill outside)
+          for (int j = 0; j < 3; j++)
+            for (int h = 0; h < 2; h++) tma_load_5d(g + (j * 2 + h) * WG_DB, &tdy, 16 * h, x0, z0, y + 1 - j, b, &full[st]);
+          for (int c = 0; c < nck; c++)
+            tma_load_5d(g + WG_A + c * WG_XS, &tin, 16 * (c0 + c), x0 - 1, z0 - 1, y, b, &full[st]);
+          issued[st]++;
+        };
+        load(0);
+        if (mine > 1) load(1);
+        for (int q = 0; q < mine && ok; q++) {
+          const int st = q & 1;
+          if (!mbar_wait(&full[st], (uint32_t)(q >> 1) & 1u, lim)) {
+            ok = false;
+            break;
+          }
+          landed[st]++;
+          tc_fence_after();
+          const uint32_t g = smem_u32(sm + st * STAGE);
+          for (int c = 0; c < nck; c++) {
+            for (int q3 = 0; q3 < 3; q3++) {  // dx = q3 - 1
+              const uint32_t acc = tmem + (uint32_t)((c * 3 + q3) * WG_N);
+#pragma unroll
+              for (int zo = 0; zo < WG_TZ; zo++) {
+#pragma unroll
+                for (int ks = 0; ks < TX / 16; ks++) {
+                  const uint64_t da = sdesc_mn_sw32(g + (uint32_t)(zo * TX + ks * 16) * 32, WG_DB);
+                  const uint64_t db = sdesc_mn_sw32(g + WG_A + (uint32_t)c * WG_XS + (uint32_t)(zo * TXS + ks * 16 + q3) * 32,
+                                                    TXS * 32);
+                  mma_bf16(acc, da, db, idesc, 1u);
+                }
+              }
+            }
+          }
+          mma_commit(&empty[st]);
+          if (q >= 1 && q + 1 < mine) {
+            // tile q + 1 reuses the stage of tile q - 1 once its MMAs are done
+            if (!mbar_wait(&empty[(q - 1) & 1], (uint32_t)((q - 1) >> 1) & 1u, lim)) {
+              ok = false;
+              break;
+            }
+            load(q + 1);
+          }
+        }
+        if (!ok) {
+          // let the copies already issued land before the shared memory is released
+          for (int st = 0; st < 2; st++)
+            for (; landed[st] < issued[st]; landed[st]++) mbar_wait(&full[st], (uint32_t)landed[st] & 1u, lim);
+        }
+      }
+      if (!ok) {
+        atomicExch(err, 1);
+        bad = 1;
+      }
+      mma_commit(&acc_full);  // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+  } else {
+    const bool ready = mbar_wait(&acc_full, 0, lim);
+    if (!ready) {
+      if (lane == 0) atomicExch(err, 1);
+      bad = 1;
+    }
+    tc_fence_after();
+    if (warp < 3 && ready && !bad && mine > 0) {
+      // TMEM lane 32 w + co holds dy = w - 1, output channel co
+      for (int c = 0; c < nck; c++)
+        for (int q3 = 0; q3 < 3; q3++)
+          for (int n0 = 0; n0 < WG_N; n0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((c * 3 + q3) * WG_N + n0), v);
+            const int tap = warp * 9 + q3 * 3 + n0 / 16;
+            float *o = dw + ((size_t)tap * s.cin + (size_t)(c0 + c) * 16) * 32 + lane;
+#pragma unroll
+            for (int i = 0; i < 16; i++) atomicAdd(o + (size_t)i * 32, v[i]);
+          }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_free(tmem, 512);
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -296,6 +482,48 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // tile height for a shape: 4 z-lines when cout <= 32 and Z allows, else 2
 static int tile_tz(const ConvShape &s) { return (s.n <= 32 && s.Z % 4 == 0) ? 4 : 2; }
+
+bool wgrad_tile_supported(const ConvShape &s) {
+  return s.nb >= 1 && s.Y >= 1 && s.X >= TX && s.X % TX == 0 && s.Z >= WG_TZ && s.Z % WG_TZ == 0 && s.cin >= 16 &&
+         s.cin % 16 == 0 && s.n == 32 && (long long)(s.X / TX) * (s.Z / WG_TZ) * s.nb * s.Y < (1ll << 31) &&
+         encode_fn() != nullptr;
+}
+
+// activations [nb][Y][X][Z][c] seen as (c, x, z, y, b), boxes of 16 channels
+static bool encode_act(CUtensorMap *m, const __nv_bfloat16 *p, const ConvShape &s, int c, int bx, int bz) {
+  const cuuint64_t C2 = (cuuint64_t)c * 2;
+  const cuuint64_t dims[5] = {(cuuint64_t)c, (cuuint64_t)s.X, (cuuint64_t)s.Z, (cuuint64_t)s.Y, (cuuint64_t)s.nb};
+  const cuuint64_t strides[4] = {(cuuint64_t)s.Z * C2, C2, (cuuint64_t)s.X * s.Z * C2, (cuuint64_t)s.Y * s.X * s.Z * C2};
+  const cuuint32_t box[5] = {16, (cuuint32_t)bx, (cuuint32_t)bz, 1, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  return encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16 *>(p), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t conv_wgrad_tile(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, float *dw,
+                            int *err, cudaStream_t st) {
+  if (!wgrad_tile_supported(s)) return cudaErrorNotSupported;
+  CUtensorMap mi, md;
+  if (!encode_act(&mi, in, s, s.cin, TXS, WG_TZ + 2) || !encode_act(&md, dout, s, s.n, TX, WG_TZ))
+    return cudaErrorNotSupported;
+  const int nchunk = s.cin / 16, cpg = std::min(nchunk, WG_CPG);
+  const int groups = (nchunk + cpg - 1) / cpg;
+  static int sms = 0;
+  cudaError_t e;
+  if (!sms) {
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  }
+  const long long ntiles = (long long)(s.X / TX) * (s.Z / WG_TZ) * s.nb * s.Y;
+  const int slices = (int)std::max(1ll, std::min(ntiles, (long long)std::max(1, sms / groups)));
+  const size_t smem = 2 * (size_t)wg_stage(cpg) + WG_SLACK;
+  e = cudaFuncSetAttribute((const void *)k_wgrad_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_wgrad_tile<<<(unsigned)(groups * slices), 160, smem, st>>>(mi, md, s, dw, slices, err);
+  return cudaGetLastError();
+}
 
 bool conv_tile_supported(const ConvShape &s) {
   return s.nb >= 1 && s.Y >= 1 && s.X >= TX && s.X % TX == 0 && s.Z >= 2 && s.Z % 2 == 0 && s.cin >= 8 &&

@@ -28,8 +28,15 @@ cudaError_t conv_tile_pack(int cin, int n, int kpad, int sign, const __nv_bfloat
                            cudaStream_t st);
 cudaError_t conv_forward_tile(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *wp, const float *bias,
                               void *out, int epi, int sign, int *err, cudaStream_t st);
+// weight gradient: the TMA tile kernel where wgrad_tile_supported (cout 32,
+// cin a multiple of 16, X a multiple of 128, Z even), else the gather kernel;
+// path 1 forces the gather kernel, 2 the tile kernel (cudaErrorNotSupported
+// where it does not apply)
 cudaError_t conv_wgrad(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, float *dw, int *err,
-                       cudaStream_t st);
+                       cudaStream_t st, int path = 0);
+bool wgrad_tile_supported(const ConvShape &s);
+cudaError_t conv_wgrad_tile(const ConvShape &s, const __nv_bfloat16 *in, const __nv_bfloat16 *dout, float *dw,
+                            int *err, cudaStream_t st);
 
 void pack_input(long long nv, const float *a, const float *b, float scale, __nv_bfloat16 *out, cudaStream_t st);
 void avgpool(int nb, int Y, int X, int Z, int C, const __nv_bfloat16 *in, __nv_bfloat16 *out, cudaStream_t st);

@@ -39,8 +39,8 @@ XTG_SYMBOLS = [
     "xtg_nhicd_threshold_noalloc",
 ]
 # warm-start network entry points (include/xtg_cnn.h), also in libxtgpu.so
-XTC_SYMBOLS = ["xtc_wait_selftest", "xtc_conv3d", "xtc_conv3d_path", "xtc_conv3d_wgrad", "xtc_net_create", "xtc_net_destroy", "xtc_net_param_count",
-               "xtc_net_get_params", "xtc_net_set_params", "xtc_net_save", "xtc_net_load", "xtc_net_forward",
+XTC_SYMBOLS = ["xtc_wait_selftest", "xtc_conv3d", "xtc_conv3d_path", "xtc_conv3d_wgrad", "xtc_conv3d_wgrad_path",
+               "xtc_net_create", "xtc_net_destroy", "xtc_net_param_count", "xtc_net_get_params", "xtc_net_set_params", "xtc_net_save", "xtc_net_load", "xtc_net_forward",
                "xtc_net_backward", "xtc_net_adam_step", "xtc_net_train", "xtg_init_object_learned"]
 XTGEN_SYMBOLS = [
     "xtgen_views_uniform", "xtgen_views_interlaced", "xtgen_write_view_file", "xtgen_phantom",
