@@ -3,7 +3,9 @@ PyTorch fp32 reference on the CPU (same BF16-rounded inputs and weights).
 
 Both kernels are covered: the gather kernel (operands gathered per K stage)
 and the tile kernel (the input tile staged once by TMA, each tap a shifted
-shared-memory view; X a multiple of 128, Z even, cout <= 64).
+shared-memory view; X a multiple of 128, Z even, cout <= 64), and both
+weight gradients (gather; TMA tiles with the dy taps along M and the dz taps
+along N, cout 32).
 
 Tolerance: FP32 accumulation in a different order over K = 27*cin terms,
 |got - ref| <= 1e-4 * max|ref| (FP32 output), plus one BF16 rounding of the
