@@ -195,39 +195,52 @@ __global__ void k_amatrix_batch(DevGeo G, const float *hr, const float *cosv, co
 // halo_hi (z slab with a neighbour above): the pairs from the top slice into
 // that neighbour's bottom slice belong to this slab's sum, as the reference's
 // ranks other than the last include Object[i][N_z+1] (XT_ICD_update.c:203-205).
-__global__ void k_prior_cost64(DevGeo G, const float *x, const float *halo_hi, double *slots) {
-  const size_t n = (size_t)G.N_time * G.N_y * G.N_x * G.N_z;
+__global__ void __launch_bounds__(256, 3) k_prior_cost64(DevGeo G, const float *x, const float *halo_hi, double *slots) {
+  // one warp per z-line (f, j, k), lanes over z: the line's coordinates are
+  // decoded once, every load is a coalesced run of the line
+  const long long nlines = (long long)G.N_time * G.N_y * G.N_x;
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  // rho(d) = (d^2 / sq) / (c + |d|^(2-p) / sqp) evaluated as
+  // d^2 / (sq c + (sq / sqp) 2^((2-p) log2 |d|)): one division, and
+  // log2 / exp2 in place of pow (the same value to a few ulp)
+  const double ks1 = (double)G.Sigma_S_Q * G.C_S, ks2 = (double)G.Sigma_S_Q / G.Sigma_S_Q_P;
+  const double kt1 = (double)G.Sigma_T_Q * G.C_T, kt2 = (double)G.Sigma_T_Q / G.Sigma_T_Q_P;
+  const double e2p = 2.0 - (double)G.MRF_P;
+  auto rho = [&](double d, double k1, double k2) -> double {
+    const double a = fabs(d);
+    return a == 0.0 ? 0.0 : (a * a) / (k1 + k2 * exp2(e2p * log2(a)));
+  };
+  const size_t plane = (size_t)G.N_y * G.N_x;
   double acc = 0.0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int z = (int)(i % G.N_z);
-    size_t r = i / G.N_z;
-    const int k = (int)(r % G.N_x);
-    r /= G.N_x;
+  for (long long L = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); L < nlines; L += nwarps) {
+    const int k = (int)(L % G.N_x);
+    const long long r = L / G.N_x;
     const int j = (int)(r % G.N_y);
     const int f = (int)(r / G.N_y);
-    const double v = x[i];
-    const double sq = G.Sigma_S_Q, sqp = G.Sigma_S_Q_P, cs = G.C_S, pp = G.MRF_P;
-    auto X = [&](int ff, int jj, int kk, int zz) -> double {
-      if (zz == G.N_z) return (double)halo_hi[((size_t)ff * G.N_y + jj) * G.N_x + kk];
-      return (double)x[(((size_t)ff * G.N_y + jj) * G.N_x + kk) * G.N_z + zz];
-    };
-    auto term = [&](int dz, int dy, int dx) {
-      const int jj = j + dy, kk = k + dx, zz = z + dz;
-      if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x || (zz >= G.N_z && !halo_hi)) return;
-      acc += (double)G.SF[(1 + dz) * 9 + (1 + dy) * 3 + (1 + dx)] * xt_qggmrf_value64(v - X(f, jj, kk, zz), sq, sqp, cs, pp);
-    };
-    term(0, 0, 1);
-    term(0, 1, -1);
-    term(0, 1, 0);
-    term(0, 1, 1);
-    for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) term(1, dy, dx);
-    if (f + 1 < G.N_time)
-      acc += (double)G.TF * xt_qggmrf_value64(v - X(f + 1, j, k, z), G.Sigma_T_Q, G.Sigma_T_Q_P, G.C_T, pp);
+    const float *xl = x + (size_t)L * G.N_z;
+    for (int z = lane; z < G.N_z; z += 32) {
+      const double v = xl[z];
+      auto term = [&](int dz, int dy, int dx) {
+        const int jj = j + dy, kk = k + dx, zz = z + dz;
+        if (jj < 0 || jj >= G.N_y || kk < 0 || kk >= G.N_x || (zz >= G.N_z && !halo_hi)) return;
+        const long long off = (long long)dy * G.N_x + dx;
+        const double u = zz == G.N_z ? (double)halo_hi[(size_t)(L + off)] : (double)xl[off * G.N_z + zz];
+        acc += (double)G.SF[(1 + dz) * 9 + (1 + dy) * 3 + (1 + dx)] * rho(v - u, ks1, ks2);
+      };
+      term(0, 0, 1);
+      term(0, 1, -1);
+      term(0, 1, 0);
+      term(0, 1, 1);
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) term(1, dy, dx);
+      if (f + 1 < G.N_time)
+        acc += (double)G.TF * rho(v - (double)xl[plane * G.N_z + z], kt1, kt2);
+    }
   }
   __shared__ double red[32];
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  if (lane == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0;
@@ -1463,7 +1476,9 @@ int xtg_resync_fp64(xtg_ctx *c, double *cost, double *fwd, double *prior) {
 
 static int finish_cost(xtg_ctx *c, double data_sum, double *cost, double *fwd, double *prior) {
   CK(cudaMemsetAsync(c->d_red + NSLOT, 0, NSLOT * 8, c->st));
-  const unsigned grid = std::min<unsigned>(blocks_for(c->nvox, 256), (unsigned)c->sm_count * 8);
+  // one warp per z-line, 8 warps per CTA
+  const unsigned grid = std::min<unsigned>(blocks_for((size_t)c->g.N_time * c->g.N_y * c->g.N_x, 8),
+                                           (unsigned)c->sm_count * 8);
   k_prior_cost64<<<grid, 256, 0, c->st>>>(c->G, c->d_x, c->halo_hi, c->d_red + NSLOT);
   c->launches++;
   CK(cudaGetLastError());

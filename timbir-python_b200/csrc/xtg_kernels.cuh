@@ -204,11 +204,6 @@ __device__ __forceinline__ float xt_qggmrf_coef(float d, float sq, float sqp, fl
   return (2.0f - (2.0f - p) * t1 / t3) / (t3 * sq);
 }
 
-__device__ __forceinline__ double xt_qggmrf_value64(double d, double sq, double sqp, double c, double p) {
-  const double a = fabs(d);
-  return (a * a / sq) / (c + pow(a, 2.0 - p) / sqp);
-}
-
 // red.global.add on four consecutive floats: no lost updates when two
 // columns in flight share sinogram entries.
 __device__ __forceinline__ void xt_red_add4(float *p, float a, float b, float c, float d) {
