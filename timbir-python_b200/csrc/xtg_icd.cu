@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     return sGrab[0] + sGrab[1]++;
   };
   auto item_index = [&](int i) -> int {
-    const int ii = i % nitems;
+    const int ii = A.nsub == 1 ? i : i % nitems;
     return A.item_lo + (A.use_perm ? (int)xt_perm((uint32_t)ii, (uint32_t)nitems, A.perm_key) : ii);
   };
   // the rank and run-bound steps with plain loads (prologue, skipped pieces)
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     __syncthreads();
     const int it = PF ? sMeta[mb].it : sItem;
     if (it >= total) break;
-    const int piece = it / nitems;
+    const int piece = A.nsub == 1 ? 0 : it / nitems;
     const int4 item = PF ? sMeta[mb].item : A.items[item_index(it)];
     const int fr = item.x, row = item.y, col = item.z, blk = item.w;
     int zb = 0, ze = G.N_z - 1;
@@ -292,8 +292,19 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
         cp_async4(&sEnt[e].y, A.tval32 + s0 + e);
       }
     }
+    // Zero skipping (XT_VoxUpdate.c:208-232) decided for the whole z-line
+    // before any footprint work: from the second iteration a voxel equal to 0
+    // with no positive spatial or temporal neighbour is not updated.  When
+    // that holds for every voxel of the item, theta is never used, so neither
+    // A nor the footprint is read (the update step below skips each voxel by
+    // the same test and the e update has nothing to add).  Each thread tests
+    // the values it stages.
+    bool quiet = A.iter > 1;
+    // k / (Z + 2) as (k * mz2) >> 20: exact while k (Z + 2) < 2^20, and here
+    // k < 9 (Z + 2) with Z + 2 <= 130
+    const uint32_t z2 = (uint32_t)Z + 2u, mz2 = ((1u << 20) + z2 - 1u) / z2;
     for (int k = tid; k < 9 * (Z + 2); k += NT) {
-      const int c = k / (Z + 2), zz = k - c * (Z + 2);
+      const int c = (int)(((uint32_t)k * mz2) >> 20), zz = k - c * (Z + 2);
       const int jj = row + c / 3 - 1, kk = col + c % 3 - 1, za = zb - 1 + zz;
       float v = 0.f;
       if (jj >= 0 && jj < G.N_y && kk >= 0 && kk < G.N_x) {
@@ -306,29 +317,15 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
           v = A.halo_hi[q];
       }
       sNb[c * (zmax + 2) + zz] = v;
+      const bool self = (c == 4) && zz >= 1 && zz <= Z;
+      if (self ? (v != 0.f) : (v > 0.f)) quiet = false;
     }
     for (int k = tid; k < 2 * Z; k += NT) {
-      const int s = k / Z, z = k - s * Z, f2 = fr + (s ? 1 : -1);
+      const int s = k >= Z ? 1 : 0, z = k - s * Z, f2 = fr + (s ? 1 : -1);
       float v = 0.f;
       if (f2 >= 0 && f2 < G.N_time) v = A.x[(((size_t)f2 * plane) + (size_t)row * G.N_x + col) * G.N_z + zb + z];
       sTn[s * zmax + z] = v;
-    }
-    // Zero skipping (XT_VoxUpdate.c:208-232) decided for the whole z-line
-    // before any footprint work: from the second iteration a voxel equal to 0
-    // with no positive spatial or temporal neighbour is not updated.  When
-    // that holds for every voxel of the item, theta is never used, so neither
-    // A nor the footprint is read (the update step below skips each voxel by
-    // the same test and the e update has nothing to add).
-    bool quiet = A.iter > 1;
-    if (quiet) {
-      for (int k = tid; k < 9 * (Z + 2); k += NT) {
-        const int c = k / (Z + 2), zz = k - c * (Z + 2);
-        const float v = sNb[c * (zmax + 2) + zz];
-        const bool self = (c == 4) && zz >= 1 && zz <= Z;
-        if (self ? (v != 0.f) : (v > 0.f)) quiet = false;
-      }
-      for (int k = tid; k < 2 * Z; k += NT)
-        if (sTn[(k / Z) * zmax + k % Z] > 0.f) quiet = false;
+      if (v > 0.f) quiet = false;
     }
     const bool skip_all = __syncthreads_and(quiet) != 0;
     // 2. the column's A entries (times delta_t, XT_VoxUpdate.c:27) -> smem
