@@ -372,10 +372,10 @@ def network_train(nxy, nz, steps, patch, batch=8, volumes=4):
     dt = time.perf_counter() - t0
     vox = batch * patch[0] * patch[1] * patch[2]
     flops = 3 * sum(2.0 * 27 * ci * co * vox / 8 ** lvl for ci, co, lvl in NET_LAYERS)
-    print(json.dumps({"network_train": {"patch": list(patch), "batch": batch, "steps": steps},
-                      "ms_per_step": dt * 1e3 / steps, "tflops": flops * steps / dt / 1e12,
-                      "loss_last20": float(losses[-20:].mean())}), flush=True)
     net.close()
+    return {"network_train": {"patch": list(patch), "batch": batch, "steps": steps, "volumes": [nxy, nxy, nz]},
+            "ms_per_step": dt * 1e3 / steps, "tflops": flops * steps / dt / 1e12,
+            "loss_last20": float(losses[-20:].mean())}
 
 
 def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, coarse_iters=30, learned=True,
@@ -477,6 +477,9 @@ def converge(ctx, amode, tol=1e-4, max_iters=400, stall=1e-7, resync_every=10, c
     if net is not None:
         out["network"] = network_roofline(ctx, net, coarse_iters)
         net.close()
+        # training throughput of the same network with the library's own
+        # forward / backward / Adam kernels (wall clock around the steps)
+        out["network"]["training"] = network_train(256, 32, 100, (32, 128, 32))
     ctx.set_options(a_mode=AMODES[amode])
     z = out.get("zero", {}).get("s")
     for k in ("fbp", "multires", "learned"):
@@ -952,7 +955,7 @@ def main():
     if args.network_forward:
         network_forward(args.nxy or 512, args.nz, args.reps)
     elif args.network_train:
-        network_train(args.nxy or 256, args.nz, args.steps, args.patch)
+        print(json.dumps(network_train(args.nxy or 256, args.nz, args.steps, args.patch)), flush=True)
     elif args.kernels:
         kernel_timings(args)
     elif args.impl == "reference":
