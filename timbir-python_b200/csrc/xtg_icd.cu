@@ -390,11 +390,11 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     // one footprint entry: rows [off, off + VEC) past this thread's first row
     // of one (view, bin), weight a.  Generalized-Huber (zinger) weight
     // (XT_VoxUpdate.c:34-48): w where |e sqrt(w)| < T, else
-    // we = T delta sqrt(w) / |e|, so that
+    // we = T delta sqrt(w) / |e| = T delta w rsqrt(e^2 w), so that
     //   theta2 += a^2 we = a^2 T delta sqrt(w) / |e|,
     //   theta1 -= a e we = a T delta sign(e) sqrt(w);
-    // sqrt(w) = w rsqrt(w) and 1/|e| come from the special-function unit, and
-    // the branch runs only when some lane of the warp meets a zinger.
+    // rsqrt comes from the special-function unit, and the weighted branch
+    // runs only when some lane of the warp meets a zinger.
     const int trow0 = t0 + tl * VEC;
     const float *eb = A.e + trow0;
     const float *wb = A.w + trow0;
@@ -409,16 +409,13 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
         qm = fmaxf(qm, q[c]);
       }
       if (__any_sync(__activemask(), qm >= A.T2)) {
+        // branch-free per row: the weight is w, or T delta w / sqrt(e^2 w)
+        // (= T delta sqrt(w) / |e|) where |e sqrt(w)| >= T
 #pragma unroll
         for (int c = 0; c < VEC; c++) {
-          if (q[c] >= A.T2) {
-            const float sw = wv[c] * rsqrtf(wv[c]);
-            th2[c] = fmaf(a2 * A.Tdelta, __fdividef(sw, fabsf(ev[c])), th2[c]);
-            th1[c] = fmaf(na * A.Tdelta, copysignf(sw, ev[c]), th1[c]);
-          } else {
-            th2[c] = fmaf(a2, wv[c], th2[c]);
-            th1[c] = fmaf(na, ew[c], th1[c]);
-          }
+          const float we = q[c] >= A.T2 ? A.Tdelta * wv[c] * rsqrtf(q[c]) : wv[c];
+          th2[c] = fmaf(a2, we, th2[c]);
+          th1[c] = fmaf(na, ev[c] * we, th1[c]);
         }
       } else {
 #pragma unroll
