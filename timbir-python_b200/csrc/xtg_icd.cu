@@ -94,6 +94,12 @@ struct ItemMeta {
 
 // Footprint entries a thread loads before it uses any of them (table modes,
 // 16-byte rows): more loads in flight per warp to cover L2/HBM latency.
+// Packed FP32 (two lanes per instruction, sm_100) for the footprint
+// arithmetic of 16-byte rows
+#ifndef XTG_F32X2
+#define XTG_F32X2 1
+#endif
+
 #ifndef XTG_UNROLL
 #define XTG_UNROLL 2
 #endif
@@ -400,6 +406,37 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
     const float *wb = A.w + trow0;
     auto accumulate_arr = [&](const float (&ev)[VEC], const float (&wv)[VEC], float a) {
       const float a2 = a * a, na = -a;
+      if constexpr (VEC == 4 && XTG_F32X2) {
+        // two rows per instruction on the packed FP32 path; every product and
+        // fused multiply-add is rounded as the scalar one would be
+        const float2 e0 = make_float2(ev[0], ev[1]), e1 = make_float2(ev[2], ev[3]);
+        const float2 w0 = make_float2(wv[0], wv[1]), w1 = make_float2(wv[2], wv[3]);
+        const float2 ew0 = __fmul2_rn(e0, w0), ew1 = __fmul2_rn(e1, w1);
+        const float2 q0 = __fmul2_rn(e0, ew0), q1 = __fmul2_rn(e1, ew1);  // e^2 w
+        const float qm = fmaxf(fmaxf(q0.x, q0.y), fmaxf(q1.x, q1.y));
+        const float2 aa = make_float2(a2, a2), nn = make_float2(na, na);
+        float2 t20 = make_float2(th2[0], th2[1]), t21 = make_float2(th2[2], th2[3]);
+        float2 t10 = make_float2(th1[0], th1[1]), t11 = make_float2(th1[2], th1[3]);
+        if (__any_sync(__activemask(), qm >= A.T2)) {
+          // the weight is w, or T delta w / sqrt(e^2 w) (= T delta sqrt(w) / |e|)
+          // where |e sqrt(w)| >= T
+          auto wgt = [&](float q, float w) { return q >= A.T2 ? A.Tdelta * w * rsqrtf(q) : w; };
+          const float2 we0 = make_float2(wgt(q0.x, w0.x), wgt(q0.y, w0.y));
+          const float2 we1 = make_float2(wgt(q1.x, w1.x), wgt(q1.y, w1.y));
+          t20 = __ffma2_rn(aa, we0, t20);
+          t21 = __ffma2_rn(aa, we1, t21);
+          t10 = __ffma2_rn(nn, __fmul2_rn(e0, we0), t10);
+          t11 = __ffma2_rn(nn, __fmul2_rn(e1, we1), t11);
+        } else {
+          t20 = __ffma2_rn(aa, w0, t20);
+          t21 = __ffma2_rn(aa, w1, t21);
+          t10 = __ffma2_rn(nn, ew0, t10);
+          t11 = __ffma2_rn(nn, ew1, t11);
+        }
+        th2[0] = t20.x; th2[1] = t20.y; th2[2] = t21.x; th2[3] = t21.y;
+        th1[0] = t10.x; th1[1] = t10.y; th1[2] = t11.x; th1[3] = t11.y;
+        return;
+      }
       float ew[VEC], q[VEC];
       float qm = 0.f;
 #pragma unroll
@@ -679,7 +716,12 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
       if (any) {
         float *ebw = A.e + trow0;
         auto scatter = [&](int off, float a) {
-          if (VEC == 4) {
+          if constexpr (VEC == 4 && XTG_F32X2) {
+            const float2 na2 = make_float2(-a, -a);
+            const float2 m0 = __fmul2_rn(na2, make_float2(dv[0], dv[1]));
+            const float2 m1 = __fmul2_rn(na2, make_float2(dv[2], dv[3]));
+            xt_red_add4(ebw + off, m0.x, m0.y, m1.x, m1.y);
+          } else if (VEC == 4) {
             xt_red_add4(ebw + off, -(a * dv[0]), -(a * dv[1]), -(a * dv[2]), -(a * dv[3]));
           } else {
 #pragma unroll
