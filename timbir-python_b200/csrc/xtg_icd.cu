@@ -92,14 +92,15 @@ struct ItemMeta {
   int pad;
 };
 
-// Footprint entries a thread loads before it uses any of them (table modes,
-// 16-byte rows): more loads in flight per warp to cover L2/HBM latency.
 // Packed FP32 (two lanes per instruction, sm_100) for the footprint
 // arithmetic of 16-byte rows
 #ifndef XTG_F32X2
 #define XTG_F32X2 1
 #endif
 
+// Footprint entries a thread loads before it uses any of them (table modes,
+// 16-byte rows): more loads in flight per warp to cover L2/HBM latency.
+// Three in the 64-thread CTAs (no spills there) measured 1 % slower.
 #ifndef XTG_UNROLL
 #define XTG_UNROLL 2
 #endif
@@ -499,18 +500,19 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
         }
       } else if (VEC == 4) {
         int e = vg;
-        for (; e + (XTG_UNROLL - 1) * vgs < ne; e += XTG_UNROLL * vgs) {
-          int2 en[XTG_UNROLL];
-          float4 e4[XTG_UNROLL], w4[XTG_UNROLL];
+        constexpr int UNR = XTG_UNROLL;
+        for (; e + (UNR - 1) * vgs < ne; e += UNR * vgs) {
+          int2 en[UNR];
+          float4 e4[UNR], w4[UNR];
 #pragma unroll
-          for (int u = 0; u < XTG_UNROLL; u++) en[u] = sEnt[e + u * vgs];
+          for (int u = 0; u < UNR; u++) en[u] = sEnt[e + u * vgs];
 #pragma unroll
-          for (int u = 0; u < XTG_UNROLL; u++) {
+          for (int u = 0; u < UNR; u++) {
             e4[u] = ld_e(eb + en[u].x);
             w4[u] = ld_w(wb + en[u].x, A.w_keep);
           }
 #pragma unroll
-          for (int u = 0; u < XTG_UNROLL; u++) accumulate_vals(e4[u], w4[u], __int_as_float(en[u].y));
+          for (int u = 0; u < UNR; u++) accumulate_vals(e4[u], w4[u], __int_as_float(en[u].y));
         }
         for (; e < ne; e += vgs) {
           const int2 en = sEnt[e];
