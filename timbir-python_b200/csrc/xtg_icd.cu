@@ -100,7 +100,8 @@ struct ItemMeta {
 
 // Footprint entries a thread loads before it uses any of them (table modes,
 // 16-byte rows): more loads in flight per warp to cover L2/HBM latency.
-// Three in the 64-thread CTAs (no spills there) measured 1 % slower.
+// Three measured equal in the 256-thread CTAs (a few bytes spilled) and 1 %
+// slower in the 64-thread ones, which keep two whatever this is set to.
 #ifndef XTG_UNROLL
 #define XTG_UNROLL 2
 #endif
@@ -500,7 +501,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_c
         }
       } else if (VEC == 4) {
         int e = vg;
-        constexpr int UNR = XTG_UNROLL;
+        constexpr int UNR = NT < XTG_THREADS ? 2 : XTG_UNROLL;
         for (; e + (UNR - 1) * vgs < ne; e += UNR * vgs) {
           int2 en[UNR];
           float4 e4[UNR], w4[UNR];
