@@ -152,11 +152,17 @@ __device__ __forceinline__ Nbr nbr_term(const DevGeo &G, const float *sNb, const
 #define XTG_PF_ALL 0
 #endif
 
+// resident 256-thread CTAs per SM the register budget is cut for (5: 48
+// registers with spills, 8 % slower on plain 3D)
+#ifndef XTG_CTAS_256
+#define XTG_CTAS_256 4
+#endif
+
 // NT threads per CTA: 256 for long z-lines; 64 where a work item is short
 // (few detector rows), so the per-item fixed work (neighbourhood, A staging,
 // barriers, the surrogate step) runs in four times as many CTAs at once.
 template <int VEC, int AMODE, int SEQ, int AS, int NT = XTG_THREADS>
-__global__ void __launch_bounds__(NT, NT == XTG_THREADS ? 4 : 1024 / NT) k_icd_columns(DevGeo G, IcdArgs A, int vmax,
+__global__ void __launch_bounds__(NT, NT == XTG_THREADS ? XTG_CTAS_256 : 1024 / NT) k_icd_columns(DevGeo G, IcdArgs A, int vmax,
                                                                                  int zmax) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NW = NT / 32;
