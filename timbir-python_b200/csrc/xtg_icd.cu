@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? XTG_CTAS_256 : 1024 / 
     const int ii = A.nsub == 1 ? i : i % nitems;
     return A.item_lo + (A.use_perm ? (int)xt_perm((uint32_t)ii, (uint32_t)nitems, A.perm_key) : ii);
   };
-  // the rank and run-bound steps with plain loads (prologue, skipped pieces)
   auto fetch_rank = [&]() {  // thread 0, the next item's record in place
     ItemMeta &N = sMeta[mb ^ 1];
     if (N.it < total) cp_async4(&N.rank, A.col_rank + N.item.y * G.N_x + N.item.z);
@@ -229,6 +228,7 @@ __global__ void __launch_bounds__(NT, NT == XTG_THREADS ? XTG_CTAS_256 : 1024 / 
       if (AMODE == 1) cp_async4(&N.sc, A.tscale + ti);
     }
   };
+  // the rank and run-bound steps with plain loads (prologue, skipped pieces)
   auto meta_finish = [&](ItemMeta &N) {
     if (N.it >= total) return;
     N.rank = A.col_rank[N.item.y * G.N_x + N.item.z];
