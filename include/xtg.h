@@ -167,6 +167,15 @@ int xtg_upload_counts(xtg_ctx *ctx, const float *bright, const float *counts, do
                       const float *d);
 int xtg_upload_object(xtg_ctx *ctx, const float *x);
 int xtg_download_object(xtg_ctx *ctx, float *x);
+/* xtg_download_object without blocking the host: the object is copied to a
+ * staging buffer of the library at once (later calls may change it), and
+ * from there to x on a second stream, overlapping the work queued next (a
+ * pinned x makes the copy asynchronous).  x is complete after
+ * xtg_download_wait, which blocks until the last such copy has arrived; do
+ * not read or reuse x before it.  A second start waits on the device for the
+ * first copy to leave the staging buffer.  No XT_Engine counterpart. */
+int xtg_download_object_start(xtg_ctx *ctx, float *x);
+int xtg_download_wait(xtg_ctx *ctx);
 int xtg_get_error_sino(xtg_ctx *ctx, float *e);
 int xtg_set_error_sino(xtg_ctx *ctx, const float *e);
 int xtg_get_weight(xtg_ctx *ctx, float *w);

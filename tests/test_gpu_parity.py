@@ -108,6 +108,31 @@ def test_projectors_agree(name):
         assert x == pytest.approx(y, rel=1e-13, abs=1e-12)
 
 
+@pytest.mark.parametrize("name", ["plain3d", "timbir4d"])
+def test_download_object_start_matches_download(name):
+    """xtg_download_object_start: the object as it was at the call reaches the
+    host after xtg_download_wait, although the device object changes at once
+    (a second start and an iteration queued behind it); equal to
+    xtg_download_object's copy bit for bit."""
+    import torch
+    c, g, _ = ctx_for(name, a_mode=xtg.XTG_A_TABLE32)
+    c.upload_sino(g["y"], g["w"])
+    x1 = np.ascontiguousarray(g["x_true"], np.float32)
+    x2 = np.ascontiguousarray(g["x_true"] * 0.5, np.float32)
+    bufs = [torch.empty(c.obj_shape, dtype=torch.float32).pin_memory() for _ in range(3)]
+    c.upload_object(x1)
+    c.download_object_start(bufs[0].data_ptr())
+    c.upload_object(x2)
+    c.download_object_start(bufs[1].data_ptr())
+    c.init_error_sino()
+    c.iteration(1)
+    c.download_object_start(bufs[2].data_ptr())
+    c.download_wait()
+    assert np.array_equal(bufs[0].numpy(), x1)
+    assert np.array_equal(bufs[1].numpy(), x2)
+    assert np.array_equal(bufs[2].numpy(), c.object())
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_error_sinogram_and_cost(name):
     c, g, _ = ctx_for(name)

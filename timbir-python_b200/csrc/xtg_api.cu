@@ -123,6 +123,11 @@ struct xtg_ctx {
   cudaStream_t st = nullptr;
   cudaStream_t st_copy = nullptr;               // host-to-device copies that overlap the projector
   cudaEvent_t ev_y = nullptr, ev_w = nullptr;  // ... and their completion on it
+  // asynchronous object download: the transposed copy in d_dl leaves on
+  // st_copy after ev_dx; ev_dl marks its arrival on the host
+  float *d_dl = nullptr;
+  cudaEvent_t ev_dx = nullptr, ev_dl = nullptr;
+  int dl_pending = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
   std::vector<cudaEvent_t> tev;  // start/stop pairs of the ICD launches of one iteration
   int have_sino = 0;
@@ -760,8 +765,12 @@ void xtg_destroy(xtg_ctx *c) {
                   c->d_view_num, c->d_fov, c->d_mcols, c->d_rank, c->d_counter, c->d_nhcnt, c->d_err, c->d_kth,
                   c->d_items, c->d_nh, c->d_red, c->d_absx, c->d_cnt, c->d_tstart, c->d_toff, c->d_tval32,
                   c->d_tscale, c->d_tval16, c->d_rs_hist, c->d_rs_st, c->d_cptr, c->d_cent};
+  if (c->dl_pending && c->ev_dl) cudaEventSynchronize(c->ev_dl);
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (c->d_dl) cudaFree(c->d_dl);
+  if (c->ev_dx) cudaEventDestroy(c->ev_dx);
+  if (c->ev_dl) cudaEventDestroy(c->ev_dl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ek0) cudaEventDestroy(c->ek0);
@@ -1329,6 +1338,38 @@ int xtg_download_object(xtg_ctx *c, float *x) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(x, c->d_tmp, c->nvox * 4, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// The object leaves for the host without blocking it: transposed into its own
+// staging buffer on the engine's stream (later kernels may change x at once),
+// then copied on the copy stream, so the copy overlaps whatever the host
+// queues next (the next sinogram's upload and projection).  A second call
+// first waits for the previous copy to leave the staging buffer.
+int xtg_download_object_start(xtg_ctx *c, float *x) {
+  if (!c || !x) return XTG_E_ARG;
+  if (!c->st_copy) CK(cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
+  if (!c->ev_dx) CK(cudaEventCreateWithFlags(&c->ev_dx, cudaEventDisableTiming));
+  if (!c->ev_dl) CK(cudaEventCreateWithFlags(&c->ev_dl, cudaEventDisableTiming));
+  if (!c->d_dl && dalloc(c, &c->d_dl, c->nvox)) return XTG_E_CUDA;
+  if (c->dl_pending) CK(cudaStreamWaitEvent(c->st, c->ev_dl, 0));
+  k_obj_d2h<<<std::min<unsigned>(blocks_for(c->nvox, 256), 8192), 256, 0, c->st>>>(c->G, c->d_x, c->d_dl);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev_dx, c->st));
+  CK(cudaStreamWaitEvent(c->st_copy, c->ev_dx, 0));
+  CK(cudaMemcpyAsync(x, c->d_dl, c->nvox * 4, cudaMemcpyDeviceToHost, c->st_copy));
+  CK(cudaEventRecord(c->ev_dl, c->st_copy));
+  c->dl_pending = 1;
+  return 0;
+}
+
+int xtg_download_wait(xtg_ctx *c) {
+  if (!c) return XTG_E_ARG;
+  if (c->dl_pending) {
+    CK(cudaEventSynchronize(c->ev_dl));
+    c->dl_pending = 0;
+  }
   return 0;
 }
 

@@ -36,7 +36,7 @@ XTG_SYMBOLS = [
     "xtg_resync_fp64", "xtg_map_cost_fp64", "xtg_map_cost_running", "xtg_zinger_refresh",
     "xtg_icd_iteration", "xtg_update_columns", "xtg_nhicd_select", "xtg_update_offset",
     "xtg_update_variance", "xtg_device_bytes", "xtg_launch_count", "xtg_last_kernel_time",
-    "xtg_nhicd_threshold_noalloc",
+    "xtg_nhicd_threshold_noalloc", "xtg_download_object_start", "xtg_download_wait",
 ]
 # warm-start network entry points (include/xtg_cnn.h), also in libxtgpu.so
 XTC_SYMBOLS = ["xtc_wait_selftest", "xtc_conv3d", "xtc_conv3d_path", "xtc_conv3d_wgrad", "xtc_conv3d_wgrad_path",
@@ -402,6 +402,15 @@ class Context:
         out = np.zeros(self.obj_shape, np.float32)
         _check(self.lib.xtg_download_object(self.h, _p(out)), "xtg_download_object")
         return out
+
+    def download_object_start(self, ptr):
+        """Start copying the object to host memory at `ptr` (an address, e.g.
+        a pinned torch tensor's data_ptr(), of obj_shape float32 values);
+        complete after download_wait()."""
+        _check(self.lib.xtg_download_object_start(self.h, C.c_void_p(ptr)), "xtg_download_object_start")
+
+    def download_wait(self):
+        _check(self.lib.xtg_download_wait(self.h), "xtg_download_wait")
 
     def _get(self, fn, shape):
         out = np.zeros(shape, np.float32)
