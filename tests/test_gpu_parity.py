@@ -297,21 +297,25 @@ def test_parallel_icd_converges_to_oracle(name, amode, zslab):
     assert rmse / float(np.abs(xstar).max()) < bound
 
 
-# (parameters, oracle iterations to its converged cost)
+# (parameters, oracle iterations to its converged cost, interlaced views
+# (K, N_theta) or None, moving ellipsoids)
 ITEM_CASES = {
     # 24 detector rows, runs of ~40 entries (two frames of 20 views): 128-thread CTAs
-    "medium": (dict(N=24, NT=24, NP=40, n_time=2, nhicd=True), 120),
+    "medium": (dict(N=24, NT=24, NP=40, n_time=2, nhicd=True), 120, None, 0),
     # 18 detector rows, runs of ~1100 entries (512 views): 256-thread CTAs
-    "long": (dict(N=24, NT=18, NP=512, nhicd=True), 30),
+    "long": (dict(N=24, NT=18, NP=512, nhicd=True), 30, None, 0),
+    # 4D at 64^2 x 8 x 4 frames: 4 interlaced sub-frames of 32 views, moving
+    # and growing ellipsoids, temporal prior: 64-thread CTAs
+    "4d_64": (dict(N=64, NT=8, NP=128, n_time=4, nhicd=True), 30, (4, 32), 2),
 }
 
 
 @functools.lru_cache(maxsize=None)
 def items_case(kind):
-    kw, iters = ITEM_CASES[kind]
+    kw, iters, inter, moving = ITEM_CASES[kind]
     p = common.params(**kw)
-    t, a = common.views(p)
-    _, _, y, w = common.data(p, t, a, seed=9)
+    t, a = common.views(p, inter)
+    _, _, y, w = common.data(p, t, a, seed=9, moving=moving)
     o = Oracle(p, t, a, double=True)
     o.set_sino(y, w)
     o.init_error_sino()
@@ -322,18 +326,21 @@ def items_case(kind):
 
 
 @pytest.mark.parametrize("kind,amode", [("medium", xtg.XTG_A_TABLE32), ("medium", xtg.XTG_A_FP16),
-                                        ("long", xtg.XTG_A_TABLE32), ("long", xtg.XTG_A_FP16)])
+                                        ("long", xtg.XTG_A_TABLE32), ("long", xtg.XTG_A_FP16),
+                                        ("4d_64", xtg.XTG_A_TABLE32), ("4d_64", xtg.XTG_A_FP16)])
 def test_parallel_icd_longer_items_converge(kind, amode):
     """Work items of more than 16 detector rows in the table modes: columns
     whose runs hold at most 1024 entries run in 128-thread CTAs that take
     eight items per atomic, longer ones in 256-thread CTAs; both fetch the
-    next item's table run ahead.  The parallel schedule reaches the FP64
-    oracle's converged cost within 1e-4 relative, RMSE below 2 % of the
-    object's range."""
+    next item's table run ahead.  And a 4D case larger than the golden ones
+    (64^2 x 8, four frames of interlaced views, moving objects) in the
+    64-thread CTAs.  The parallel schedule reaches the FP64 oracle's
+    converged cost within 1e-4 relative, RMSE below 2 % of the object's
+    range."""
     p, t, a, y, w, cstar, xstar = items_case(kind)
     c = xtg.Context(p, t, a)
     c.set_options(a_mode=amode)
-    assert c.N_z * c.zovl > 16
+    assert (c.N_z * c.zovl > 16) == (kind != "4d_64")
     c.upload_sino(y, w)
     c.init_error_sino()
     for it in range(1, 61):
