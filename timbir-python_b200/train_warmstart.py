@@ -2,7 +2,7 @@
 by this engine, and saves its weights.
 
     python timbir-python_b200/train_warmstart.py --out timbir-python_b200/weights/warmstart_plain3d.bin \
-        --n 512 --nt 64 --views 1024 --volumes 24 --target-iters 30
+        --n 512 --nt 64 --views 1024 --volumes 24 --target-iters 30 --steps 6000 --patch 32 128 32
 
 (the committed weights; their .json records the run).  Training set: seeded
 ellipsoid phantoms of N^2 x NT voxels (default 256^2 x 32 with 512 views;
@@ -13,8 +13,9 @@ up, distinct from the benchmark's.  For each phantom the GPU
 engine forms the network's inputs, the FBP image and the multi-resolution
 start (`coarse_iters` ICD iterations on the 2x coarser grid, upsampled), and
 the target, the reconstruction after `target_iters` further iterations on
-the fine grid.  Training: Adam (lr 1e-3), batches of random
-64 x 64 x 32 patches.  Data generation and training run on the GPU through
+the fine grid.  Training: Adam (lr 1e-3), batches of random patches
+(default 64 x 64 x 32; the committed weights: 32 x 128 x 32, whose first
+level runs on the TMA tile kernels).  Data generation and training run on the GPU through
 the library; the host only draws the Poisson counts and sequences calls.
 """
 import argparse
